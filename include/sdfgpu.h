@@ -1,0 +1,157 @@
+/*
+ * sdfgpu.h -- C ABI of libsdfgpu.so, the B200 (sm_100a) implementation of the SignedDistances
+ * hot path of stl2sdf.jl: the truncated unsigned distance from every grid node to a triangle
+ * mesh and the ray-cast inside/outside sign.
+ *
+ * Reference interfaces replaced (paths relative to the stl2sdf.jl project):
+ *   evalDistancesOnTriMesh(mesh, grid, points) -> (dist, xp)
+ *       src/SignedDistances/dfOnTriangularMesh.jl:19        -> sdfgpu_distances
+ *   raycast_sign_detection(mesh, grid, points; min_rays=6, max_rays=30,
+ *                          confidence_threshold=0.6, use_winding_fallback=true)
+ *       src/SignedDistances/RaycastingSignDetection.jl:337  -> sdfgpu_signs
+ *   sdf_dists = dists .* signs
+ *       src/stl_to_sdf.jl:119                              -> sdfgpu_sdf (fused)
+ *   TriangularMesh(X, IEN)
+ *       src/MeshGrid/MeshInformations.jl:68                -> sdfgpu_set_mesh
+ *   Grid(AABB_min, AABB_max, N_max, margineCells)
+ *       src/MeshGrid/Grid.jl:9                             -> sdfgpu_grid_setup
+ *   noninteractive_sdf_grid_setup(mesh, B)
+ *       src/MeshGrid/Grid_setup.jl:104                     -> sdfgpu_grid_from_cell_size
+ *
+ * Conventions
+ *   - Grid nodes are implicit: node (i, j, k), 0 <= i <= N[0] etc., sits at
+ *     origin + h * [i, j, k] (one multiply and one add per component, no FMA, as Grid.jl:90),
+ *     and its linear index is i + (N[0]+1) * (j + (N[1]+1) * k) (x fastest, Grid.jl:87-89).
+ *     origin is the padded AABB_min of the reference Grid and h its cell_size.
+ *   - X is the reference's 3 x nnp column-major Float64 matrix (vertex-major: x,y,z of vertex
+ *     1, then vertex 2, ...).  IEN is the 3 x nel column-major Int64 matrix of 1-based indices.
+ *   - The caller owns every host buffer passed in or out; the library owns the device memory
+ *     held by a context.  Output buffers hold ngp = prod(N+1) doubles (xp: 3*ngp).
+ *   - Every entry point returns an sdfgpu_status; 0 is success.  sdfgpu_last_error() gives the
+ *     message of the last failure on that context.
+ *   - A context is bound to one CUDA device and is not thread safe: use one host thread per
+ *     context.  Host-buffer calls return after the results are in the host buffers.
+ *   - Sign convention of the reference: +1 inside, -1 outside.
+ */
+#ifndef SDFGPU_H
+#define SDFGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SDFGPU_ABI_VERSION 1
+
+typedef struct sdfgpu_ctx sdfgpu_ctx;
+
+typedef enum sdfgpu_status {
+  SDFGPU_OK = 0,
+  SDFGPU_ERR_INVALID_ARGUMENT = 1,
+  SDFGPU_ERR_NO_DEVICE = 2,
+  SDFGPU_ERR_CUDA = 3,
+  SDFGPU_ERR_OUT_OF_MEMORY = 4,
+  SDFGPU_ERR_NO_MESH = 5,
+  SDFGPU_ERR_CAPACITY = 6, /* a bounded per-thread buffer or traversal stack overflowed */
+  SDFGPU_ERR_IO = 7
+} sdfgpu_status;
+
+typedef enum sdfgpu_distance_mode {
+  /* The reference's rule (dfOnTriangularMesh.jl:79-177): candidates are the triangles whose
+   * centroid lies within 2.5*cell_size (else the triangles of the 3 nearest vertices), folded in
+   * ascending triangle index with the reference's vertex-skip rule, then clamped to cell_size. */
+  SDFGPU_MODE_REF_RULE = 0,
+  /* True point-triangle minimum over all triangles, clamped to cell_size. */
+  SDFGPU_MODE_EXACT = 1,
+  /* True point-triangle minimum over all triangles, not clamped (a full unsigned distance). */
+  SDFGPU_MODE_UNBOUNDED = 2
+} sdfgpu_distance_mode;
+
+typedef struct sdfgpu_opts {
+  int32_t device;  /* CUDA device ordinal */
+  int32_t tile[3]; /* nodes per distance tile along x, y, z; 0 = default / autotuned */
+} sdfgpu_opts;
+
+/* Counters of the last sdfgpu_distances / sdfgpu_signs / sdfgpu_sdf call. */
+typedef struct sdfgpu_stats {
+  int64_t ngp;                    /* grid nodes of the call */
+  int64_t nel;                    /* triangles of the mesh */
+  int64_t tile_pairs;             /* (tile, triangle) candidate pairs */
+  int64_t active_tiles;           /* tiles with at least one candidate */
+  int64_t candidate_nodes;        /* nodes whose candidate set was non-empty */
+  int64_t fp64_evals;             /* FP64 point-triangle evaluations (near-tie band) */
+  int64_t knn_fallback_nodes;     /* nodes resolved by the 3-nearest-vertex fallback */
+  int64_t band_nodes;             /* nodes flagged within cell_size by the band scatter */
+  int64_t row_hits;               /* axis-ray (row, triangle) hits */
+  int64_t undecided_nodes;        /* nodes whose 6 axis rays disagreed */
+  int64_t extra_rays;             /* rays cast beyond the 6 axis rays */
+  int64_t winding_nodes;          /* nodes that took the winding-number fallback */
+  int64_t winding_ambiguous;      /* winding nodes with | |w| - 0.5 | < 1e-9 */
+  int64_t unbounded_fallbacks;    /* learned-radius nodes that fell back to unbounded search */
+  double rho_max;                 /* max vertex distance from a triangle centroid */
+  double ms_distance;             /* device time of the distance stage (ms) */
+  double ms_sign;                 /* device time of the sign stage (ms) */
+  double ms_mesh;                 /* device time of the last set_mesh (ms) */
+} sdfgpu_stats;
+
+/* Context lifetime.  opts may be NULL (device 0, default tiles). */
+int sdfgpu_create(const sdfgpu_opts* opts, sdfgpu_ctx** out);
+int sdfgpu_destroy(sdfgpu_ctx* ctx);
+/* Message of the last failure on ctx, or of the last failed sdfgpu_create when ctx is NULL. */
+const char* sdfgpu_last_error(const sdfgpu_ctx* ctx);
+int sdfgpu_abi_version(void);
+
+/* Grid constructor (Grid.jl:9-32).  Writes the padded origin (AABB_min), the adjusted AABB_max,
+ * N (cells per axis), cell_size and ngp = prod(N+1).  Host arithmetic only; no device needed. */
+int sdfgpu_grid_setup(const double xmin[3], const double xmax[3], int64_t n_max, int64_t margin,
+                      double origin[3], double aabb_max[3], int64_t N[3], double* cell_size,
+                      int64_t* ngp);
+/* noninteractive_sdf_grid_setup (Grid_setup.jl:104-124): N_new = floor(max extent / B),
+ * margin 3, over the vertex bounding box of X (3 x nnp). */
+int sdfgpu_grid_from_cell_size(const double* X, int64_t nnp, double B, double origin[3],
+                               double aabb_max[3], int64_t N[3], double* cell_size, int64_t* ngp);
+
+/* TriangularMesh (MeshInformations.jl:68-83): uploads X (3 x nnp) and IEN (3 x nel, 1-based),
+ * validates the indices, prepares the per-triangle data (dfOnTriangularMesh.jl:329-368) and
+ * builds the LBVH.  The mesh stays resident until the next set_mesh or destroy. */
+int sdfgpu_set_mesh(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const int64_t* IEN, int64_t nel);
+/* Same, with X and IEN already in device memory of the context's device. */
+int sdfgpu_set_mesh_device(sdfgpu_ctx* ctx, const double* d_X, int64_t nnp, const int64_t* d_IEN,
+                           int64_t nel);
+
+/* evalDistancesOnTriMesh (dfOnTriangularMesh.jl:19-209) over the implicit grid.
+ * dist_out: ngp doubles; xp_out: 3*ngp doubles (closest points, vertex-major) or NULL.
+ * mode: sdfgpu_distance_mode.  use_learned_radius: only with SDFGPU_MODE_UNBOUNDED (0 or 1). */
+int sdfgpu_distances(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3],
+                     double* dist_out, double* xp_out, int32_t mode, int32_t use_learned_radius);
+
+/* raycast_sign_detection (RaycastingSignDetection.jl:337-404) over the implicit grid.
+ * sign_out: ngp doubles (+1 inside, -1 outside); conf_out: ngp doubles or NULL. */
+int sdfgpu_signs(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3],
+                 int32_t min_rays, int32_t max_rays, double confidence_threshold,
+                 int32_t use_winding_fallback, double* sign_out, double* conf_out);
+
+/* Fused stl_to_sdf.jl:105-119: distances, signs and sdf = dist .* sign in one call.  Any output
+ * pointer may be NULL except sdf_out. */
+int sdfgpu_sdf(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], int32_t mode,
+               int32_t min_rays, int32_t max_rays, double confidence_threshold,
+               int32_t use_winding_fallback, double* sdf_out, double* dist_out, double* sign_out,
+               double* conf_out);
+/* Same as sdfgpu_sdf with every output pointer in device memory; returns once the work is
+ * enqueued on the context's stream (see sdfgpu_get_stream) and the bounded host-side sizing
+ * reads are done.  The outputs are valid after that stream synchronizes. */
+int sdfgpu_sdf_device(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3],
+                      int32_t mode, int32_t min_rays, int32_t max_rays,
+                      double confidence_threshold, int32_t use_winding_fallback, double* d_sdf,
+                      double* d_dist, double* d_sign, double* d_conf);
+
+/* The cudaStream_t every kernel of the context runs on. */
+int sdfgpu_get_stream(sdfgpu_ctx* ctx, void** stream);
+int sdfgpu_get_stats(const sdfgpu_ctx* ctx, sdfgpu_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SDFGPU_H */

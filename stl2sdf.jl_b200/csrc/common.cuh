@@ -1,0 +1,166 @@
+// common.cuh -- context, device buffers, error handling and shared launch helpers of libsdfgpu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <unordered_map>
+
+#include "exact64.cuh"
+#include "geom32.cuh"
+#include "sdfgpu.h"
+
+namespace sdfgpu {
+
+// LBVH node: the boxes of both children (mesh-local FP32, rounded outward) and their ids.
+// A child id with the top bit set is a leaf: (id & 0x7fffffff) indexes the sorted primitives.
+struct __align__(16) BNode {
+  float4 a;  // lmin.x lmin.y lmin.z lmax.x
+  float4 b;  // lmax.y lmax.z rmin.x rmin.y
+  float4 c;  // rmin.z rmax.x rmax.y rmax.z
+  int4 d;    // left, right, parent, unused
+};
+constexpr int32_t kLeafBit = (int32_t)0x80000000;
+
+// Device counters (int64) zeroed at the start of every grid call.
+enum Counter : int {
+  C_TILE_PAIRS = 0,
+  C_ACTIVE_TILES,
+  C_CAND_NODES,
+  C_FP64,
+  C_KNN,
+  C_BAND,
+  C_ROW_HITS,
+  C_UNDECIDED,
+  C_EXTRA_RAYS,
+  C_WINDING,
+  C_WIND_AMBIG,
+  C_UNB_FALLBACK,
+  C_ERR_CAPACITY,   // per-thread buffer overflow
+  C_ERR_STACK,      // traversal stack overflow
+  C_ERR_INDEX,      // mesh index out of range
+  C_LIST_UNDECIDED, // length of the undecided-node list
+  C_LIST_WINDING,   // length of the winding list
+  C_NUM = 32
+};
+
+// Grid of one call, with the FP32 error scale of the mesh-local frame.
+struct GridP {
+  double o[3];
+  double h;
+  int64_t N[3];
+  int64_t n[3];     // nodes per axis (N + 1)
+  int64_t ngp;
+  double center[3]; // mesh-local frame origin
+  double E;         // bound on |coordinate - center| for every vertex and node
+  int32_t t[3];     // tile dims (nodes)
+  int64_t nt[3];    // tiles per axis
+  int64_t ntiles;
+};
+
+struct MeshDev {
+  int64_t nnp = 0, nel = 0;
+  double center[3] = {0, 0, 0};
+  double bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0};
+  double E = 0.0;        // max |vertex - center| (inf-norm)
+  double rho_max = 0.0;  // max vertex distance from its triangle's centroid
+  bool ine_ready = false;
+};
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+}  // namespace sdfgpu
+
+struct sdfgpu_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[6] = {};
+  std::string err;
+  int32_t tile[3] = {4, 4, 4};
+  bool has_mesh = false;
+  sdfgpu::MeshDev mesh;
+  std::unordered_map<std::string, sdfgpu::DevBuf> bufs;
+  int64_t* d_counters = nullptr;
+  int64_t h_counters[sdfgpu::C_NUM] = {};
+  sdfgpu_stats stats = {};
+};
+
+namespace sdfgpu {
+
+int fail(sdfgpu_ctx* ctx, int code, const std::string& msg);
+
+#define SDF_CUDA(ctx, call)                                                                       \
+  do {                                                                                            \
+    cudaError_t e__ = (call);                                                                     \
+    if (e__ != cudaSuccess) {                                                                     \
+      return ::sdfgpu::fail((ctx), e__ == cudaErrorMemoryAllocation ? SDFGPU_ERR_OUT_OF_MEMORY     \
+                                                                    : SDFGPU_ERR_CUDA,            \
+                            std::string(#call) + ": " + cudaGetErrorString(e__));                 \
+    }                                                                                             \
+  } while (0)
+
+#define SDF_TRY(expr)          \
+  do {                         \
+    int rc__ = (expr);         \
+    if (rc__ != 0) return rc__; \
+  } while (0)
+
+// Grow-only named device buffer; *out receives a pointer to at least `bytes` bytes.
+int scratch(sdfgpu_ctx* ctx, const char* name, size_t bytes, void** out);
+
+template <class T>
+inline int scratch_t(sdfgpu_ctx* ctx, const char* name, size_t count, T** out) {
+  void* p = nullptr;
+  int rc = scratch(ctx, name, count * sizeof(T) + 16, &p);
+  *out = (T*)p;
+  return rc;
+}
+
+template <class T>
+inline T* buf(sdfgpu_ctx* ctx, const char* name) {
+  auto it = ctx->bufs.find(name);
+  return it == ctx->bufs.end() ? nullptr : (T*)it->second.p;
+}
+
+inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+inline unsigned grid_for(int64_t n, int block, int64_t cap = 148 * 64) {
+  int64_t g = cdiv(n, block);
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (unsigned)g;
+}
+
+// Ordered integer encodings for atomic min/max of doubles.
+__device__ __forceinline__ unsigned long long dbl_ord(double x) {
+  unsigned long long u = (unsigned long long)__double_as_longlong(x);
+  return (u & 0x8000000000000000ULL) ? ~u : (u | 0x8000000000000000ULL);
+}
+__host__ __device__ inline double ord_dbl(unsigned long long u) {
+  u = (u & 0x8000000000000000ULL) ? (u & 0x7fffffffffffffffULL) : ~u;
+  double d;
+  memcpy(&d, &u, sizeof(d));
+  return d;
+}
+
+__device__ __forceinline__ void count_add(int64_t* counters, int idx, int64_t v) {
+  atomicAdd((unsigned long long*)&counters[idx], (unsigned long long)v);
+}
+
+// Fills GridP from (origin, h, N) and the current mesh frame; validates sizes.
+int make_grid(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], GridP& g);
+
+// Stage entry points (implemented in mesh.cu / distance.cu / sign.cu).
+int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const int64_t* IEN, int64_t nel,
+                          bool device_ptrs);
+int ensure_ine(sdfgpu_ctx* ctx);
+int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, double* d_dist, double* d_xp);
+int run_signs(sdfgpu_ctx* ctx, const GridP& g, int min_rays, int max_rays, double conf_thresh, int use_winding,
+              const double* d_dist, double* d_sign, double* d_conf, double* d_sdf);
+int cub_scan_i32(sdfgpu_ctx* ctx, const int32_t* in, int32_t* out, int64_t n);
+int cub_scan_i64(sdfgpu_ctx* ctx, const int64_t* in, int64_t* out, int64_t n);
+
+}  // namespace sdfgpu

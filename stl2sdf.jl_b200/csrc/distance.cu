@@ -1,0 +1,564 @@
+// distance.cu -- evalDistancesOnTriMesh (src/SignedDistances/dfOnTriangularMesh.jl:19-209).
+//
+// Reference semantics (SDFGPU_MODE_REF_RULE).  For node p the candidates are
+//   C(p) = { t : |centroid_t - p|^2 <= (2.5 h)^2 }                      (:48, :79)
+// or, when C(p) is empty, the triangles of the 3 nearest vertices (:82-94).  They are folded in
+// ascending triangle index with the reference's per-candidate step (box reject against the
+// running minimum, barycentric face test, edge feet, vertices only when no edge foot improved the
+// minimum) and the result is clamped to h (:202-206).
+//
+// B200 layout of the work:
+//   1. tile lists -- the grid is cut into tiles of T0 x T1 x T2 nodes.  One thread per triangle
+//      emits a (tile, triangle) pair for every tile its 2.5h centroid ball reaches; a stable CUB
+//      radix sort by tile keeps the triangles of each tile in ascending index, which is exactly
+//      the fold order.  No per-node sort is ever needed.
+//   2. fold -- one CTA per tile, one thread per node.  Every thread walks its tile's sorted list.
+//      FP32 does the bulk: the centroid-ball test in mesh-local coordinates and a point-triangle
+//      distance D.  A candidate with D > m + err (m = running FP64 minimum) provably cannot change
+//      the fold (every value the reference step could assign is >= D), so only candidates inside
+//      that band run the FP64 step of exact64.cuh, which replays the reference arithmetic.  Near
+//      the surface that is ~ln(|C(p)|) evaluations per node instead of |C(p)|.
+//   3. knn fallback -- only meshes whose triangles are large against h (max centroid-to-vertex
+//      distance rho >= 1.5h) can have a triangle within h of a node whose C(p) is empty.  For
+//      those meshes a triangle scatter flags the nodes within h of any triangle, and those nodes
+//      (or, when closest points are requested, every node with empty C(p)) run the 3-nearest-vertex
+//      fallback on the LBVH.  Every other node with empty C(p) has a result > h, so it is h.
+//
+// SDFGPU_MODE_EXACT uses the same tiles with lists of the triangles whose box lies within h of
+// the tile; SDFGPU_MODE_UNBOUNDED is a per-node LBVH nearest-triangle search without the clamp.
+#include <cub/cub.cuh>
+
+#include "common.cuh"
+
+namespace sdfgpu {
+
+namespace {
+
+constexpr double kBig = 1.0e10;  // abs(-1.0e10), the reference's initial running minimum
+
+__device__ __forceinline__ void node_ijk(const GridP& g, int64_t lin, int64_t& i, int64_t& j, int64_t& k) {
+  i = lin % g.n[0];
+  const int64_t r = lin / g.n[0];
+  j = r % g.n[1];
+  k = r / g.n[1];
+}
+
+__device__ __forceinline__ float3 local32(const GridP& g, const d3& p) {
+  return make_float3((float)(p.x - g.center[0]), (float)(p.y - g.center[1]), (float)(p.z - g.center[2]));
+}
+
+// Index range [lo, hi] of the nodes whose coordinate along axis a can lie in [x0, x1].
+__device__ __forceinline__ bool axis_range(const GridP& g, int a, double x0, double x1, int64_t& lo, int64_t& hi) {
+  double f0 = (x0 - g.o[a]) / g.h - 1e-6, f1 = (x1 - g.o[a]) / g.h + 1e-6;
+  f0 = fmax(f0, -1.0);
+  f1 = fmin(f1, (double)g.N[a] + 1.0);
+  if (!(f0 <= f1)) return false;
+  lo = (int64_t)ceil(f0);
+  hi = (int64_t)floor(f1);
+  if (lo < 0) lo = 0;
+  if (hi > g.N[a]) hi = g.N[a];
+  return lo <= hi;
+}
+
+// Emits (tile, triangle) pairs.  REF_RULE: tiles whose nodes can lie within R of the centroid;
+// EXACT: tiles whose nodes can lie within R of the triangle's box.
+template <bool kFill>
+__global__ void k_tile_pairs(const double4* __restrict__ cent, const TriRec64* __restrict__ rec, int64_t nel,
+                             GridP g, int mode, double R, int32_t* __restrict__ tri_cnt,
+                             const int32_t* __restrict__ tri_off, int32_t* __restrict__ tile_cnt,
+                             uint32_t* __restrict__ keys, int32_t* __restrict__ vals) {
+  for (int64_t el = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; el < nel; el += (int64_t)gridDim.x * blockDim.x) {
+    double lo[3], hi[3];
+    if (mode == SDFGPU_MODE_REF_RULE) {
+      const double4 c = cent[el];
+      lo[0] = c.x - R; hi[0] = c.x + R;
+      lo[1] = c.y - R; hi[1] = c.y + R;
+      lo[2] = c.z - R; hi[2] = c.z + R;
+    } else {
+      for (int a = 0; a < 3; ++a) { lo[a] = rec[el].bmin[a] - R; hi[a] = rec[el].bmax[a] + R; }
+    }
+    int64_t t0[3], t1[3];
+    bool empty = false;
+    for (int a = 0; a < 3; ++a) {
+      int64_t i0, i1;
+      if (!axis_range(g, a, lo[a], hi[a], i0, i1)) { empty = true; break; }
+      t0[a] = i0 / g.t[a];
+      t1[a] = i1 / g.t[a];
+    }
+    int32_t count = 0;
+    if (!empty) {
+      int32_t base = kFill ? tri_off[el] : 0;
+      for (int64_t tz = t0[2]; tz <= t1[2]; ++tz)
+        for (int64_t ty = t0[1]; ty <= t1[1]; ++ty)
+          for (int64_t tx = t0[0]; tx <= t1[0]; ++tx) {
+            if (mode == SDFGPU_MODE_REF_RULE) {
+              // ball (centre c, radius R) against the tile's node box
+              const int64_t ia[3] = {tx * g.t[0], ty * g.t[1], tz * g.t[2]};
+              const int64_t ib[3] = {min(ia[0] + g.t[0] - 1, g.N[0]), min(ia[1] + g.t[1] - 1, g.N[1]),
+                                     min(ia[2] + g.t[2] - 1, g.N[2])};
+              double s = 0.0;
+              for (int a = 0; a < 3; ++a) {
+                const double c = 0.5 * (lo[a] + hi[a]);
+                const double b0 = g.o[a] + g.h * (double)ia[a], b1 = g.o[a] + g.h * (double)ib[a];
+                const double d = c < b0 ? b0 - c : (c > b1 ? c - b1 : 0.0);
+                s += d * d;
+              }
+              if (s > R * R * (1.0 + 1e-9)) continue;
+            }
+            const uint32_t tile = (uint32_t)((tz * g.nt[1] + ty) * g.nt[0] + tx);
+            if (kFill) {
+              keys[base + count] = tile;
+              vals[base + count] = (int32_t)el;
+            } else {
+              atomicAdd(&tile_cnt[tile], 1);
+            }
+            ++count;
+          }
+    }
+    if (!kFill) tri_cnt[el] = count;
+  }
+}
+
+struct FoldArgs {
+  GridP g;
+  int mode;
+  const int32_t* tile_off;
+  const int32_t* tile_cnt;
+  const int32_t* vals;
+  const TriRec64* rec;
+  const double4* cent;
+  const float4* v32;
+  const float4* c32;
+  double r2;        // (2.5h)^2, the reference's inrange radius squared
+  float r2_in;      // FP32 squared radius below which the centroid test is certain
+  float r2_out;     // FP32 squared radius above which the centroid test certainly fails
+  float eD_abs;     // FP32 point-triangle distance error bound: eD_abs + eD_rel * m
+  float eD_rel;
+  double* dist;
+  double* xp;
+  uint8_t* status;
+  int64_t* counters;
+};
+
+__global__ void __launch_bounds__(256) k_tile_fold(FoldArgs A) {
+  const GridP& g = A.g;
+  const int64_t tile = blockIdx.x;
+  const int64_t tx = tile % g.nt[0], ty = (tile / g.nt[0]) % g.nt[1], tz = tile / (g.nt[0] * g.nt[1]);
+  const int lx = threadIdx.x % g.t[0], ly = (threadIdx.x / g.t[0]) % g.t[1], lz = threadIdx.x / (g.t[0] * g.t[1]);
+  const int64_t i = tx * g.t[0] + lx, j = ty * g.t[1] + ly, k = tz * g.t[2] + lz;
+  const bool valid = i <= g.N[0] && j <= g.N[1] && k <= g.N[2];
+  int64_t fp64 = 0;
+  int cand = 0;
+  if (valid) {
+    const int64_t lin = i + g.n[0] * (j + g.n[1] * k);
+    const d3 p = node_coord(g.o, g.h, i, j, k);
+    const float3 p32 = local32(g, p);
+    const int32_t start = A.tile_off[tile], cnt = A.tile_cnt[tile];
+    double m = kBig;
+    d3 proj = {0.0, 0.0, 0.0};
+    bool have = false, any = false;
+    const bool ref = A.mode == SDFGPU_MODE_REF_RULE;
+    for (int32_t e = start; e < start + cnt; ++e) {
+      const int32_t tri = __ldg(&A.vals[e]);
+      if (ref) {
+        const float4 c = __ldg(&A.c32[tri]);
+        const float dx = c.x - p32.x, dy = c.y - p32.y, dz = c.z - p32.z;
+        const float s32 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        if (s32 > A.r2_out) continue;
+        if (s32 >= A.r2_in) {  // inside the FP32 error band: the reference's FP64 test decides
+          const double4 cc = A.cent[tri];
+          const double ex = ds(cc.x, p.x), ey = ds(cc.y, p.y), ez = ds(cc.z, p.z);
+          double s = dm(ex, ex);
+          s = da(s, dm(ey, ey));
+          s = da(s, dm(ez, ez));
+          if (!(s <= A.r2)) continue;
+        }
+      }
+      any = true;
+      if (have) {
+        const float D = sqrtf(pt_tri_d2(p32, f3(__ldg(&A.v32[3 * tri])), f3(__ldg(&A.v32[3 * tri + 1])),
+                                        f3(__ldg(&A.v32[3 * tri + 2]))));
+        if ((double)D > m + (double)(A.eD_abs + A.eD_rel * (float)m)) continue;
+      }
+      tri_step64(A.rec[tri], p, m, proj, ref);
+      have = true;
+      ++fp64;
+    }
+    double d = m;
+    if (fabs(d) > fabs(g.h)) d = g.h;  // clamp (dfOnTriangularMesh.jl:202-206)
+    A.dist[lin] = d;
+    if (A.xp) {
+      A.xp[3 * lin] = proj.x;
+      A.xp[3 * lin + 1] = proj.y;
+      A.xp[3 * lin + 2] = proj.z;
+    }
+    A.status[lin] = any ? 1 : 0;
+    cand = any ? 1 : 0;
+  }
+  // warp-aggregated counters
+  for (int off = 16; off > 0; off >>= 1) {
+    fp64 += __shfl_down_sync(0xffffffffu, fp64, off);
+    cand += __shfl_down_sync(0xffffffffu, cand, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (fp64) count_add(A.counters, C_FP64, fp64);
+    if (cand) count_add(A.counters, C_CAND_NODES, cand);
+  }
+}
+
+// Flags the nodes within h (+ FP32 margin) of a triangle.
+__global__ void k_band(const float4* __restrict__ v32, const TriRec64* __restrict__ rec, int64_t nel, GridP g,
+                       double hb, float hb2, uint8_t* __restrict__ band) {
+  for (int64_t el = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; el < nel; el += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lo[3], hi[3];
+    bool empty = false;
+    for (int a = 0; a < 3; ++a)
+      if (!axis_range(g, a, rec[el].bmin[a] - hb, rec[el].bmax[a] + hb, lo[a], hi[a])) { empty = true; break; }
+    if (empty) continue;
+    const float3 a = f3(v32[3 * el]), b = f3(v32[3 * el + 1]), c = f3(v32[3 * el + 2]);
+    for (int64_t k = lo[2]; k <= hi[2]; ++k)
+      for (int64_t j = lo[1]; j <= hi[1]; ++j)
+        for (int64_t i = lo[0]; i <= hi[0]; ++i) {
+          const d3 p = node_coord(g.o, g.h, i, j, k);
+          if (pt_tri_d2(local32(g, p), a, b, c) <= hb2) band[i + g.n[0] * (j + g.n[1] * k)] = 1;
+        }
+  }
+}
+
+constexpr int kStack = 64;
+constexpr int kKnnCap = 256;
+
+struct KnnArgs {
+  GridP g;
+  const uint8_t* status;
+  const uint8_t* band;  // NULL: every node with an empty candidate set
+  const BNode* nodes;
+  const int32_t* leaf_prim;
+  const int32_t* tri_idx;  // not used (IEN64 is read instead)
+  const int64_t* IEN;
+  const double* X;
+  const int32_t* ine_off;
+  const int32_t* ine;
+  const TriRec64* rec;
+  float pad;
+  int64_t max_visits;
+  double* dist;
+  double* xp;
+  int64_t* counters;
+};
+
+__device__ __forceinline__ void child_box(const BNode& nd, int side, float3& lo, float3& hi) {
+  if (side == 0) {
+    lo = make_float3(nd.a.x, nd.a.y, nd.a.z);
+    hi = make_float3(nd.a.w, nd.b.x, nd.b.y);
+  } else {
+    lo = make_float3(nd.b.z, nd.b.w, nd.c.x);
+    hi = make_float3(nd.c.y, nd.c.z, nd.c.w);
+  }
+}
+
+// knn(vtx_kdtree, p, 3) + union of INE + ordered fold (dfOnTriangularMesh.jl:82-177).
+__global__ void k_knn_fallback(KnnArgs A) {
+  const GridP& g = A.g;
+  int64_t done = 0;
+  for (int64_t lin = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; lin < g.ngp; lin += (int64_t)gridDim.x * blockDim.x) {
+    if (A.status[lin]) continue;
+    if (A.band && !A.band[lin]) continue;
+    int64_t i, j, k;
+    node_ijk(g, lin, i, j, k);
+    const d3 p = node_coord(g.o, g.h, i, j, k);
+    const float3 p32 = local32(g, p);
+    double bs[3] = {INFINITY, INFINITY, INFINITY};
+    int64_t bv[3] = {-1, -1, -1};
+    int stack[kStack];
+    int sp = 0;
+    stack[sp++] = 0;
+    bool overflow = false;
+    int64_t visits = 0;
+    while (sp > 0) {
+      if (++visits > A.max_visits) { overflow = true; break; }
+      const BNode nd = A.nodes[stack[--sp]];
+      const float r = isinf(bs[2]) ? INFINITY : (float)sqrt(bs[2]) + A.pad;
+      const int ch[2] = {nd.d.x, nd.d.y};
+      for (int side = 0; side < 2; ++side) {
+        float3 lo, hi;
+        child_box(nd, side, lo, hi);
+        if (lo.x > hi.x) continue;
+        if (!isinf(r) && box_d2(p32, lo, hi) > r * r) continue;
+        if (ch[side] & kLeafBit) {
+          const int prim = A.leaf_prim[ch[side] & 0x7fffffff];
+          for (int q = 0; q < 3; ++q) {
+            const int64_t vi = A.IEN[3 * (int64_t)prim + q] - 1;
+            if (vi == bv[0] || vi == bv[1] || vi == bv[2]) continue;
+            const double dx = ds(A.X[3 * vi], p.x), dy = ds(A.X[3 * vi + 1], p.y), dz = ds(A.X[3 * vi + 2], p.z);
+            double s = dm(dx, dx);
+            s = da(s, dm(dy, dy));
+            s = da(s, dm(dz, dz));
+            // insert (s, vi) into the sorted top 3 (ties to the lower vertex index)
+            int pos = 3;
+            while (pos > 0 && (s < bs[pos - 1] || (s == bs[pos - 1] && vi < bv[pos - 1]))) --pos;
+            if (pos < 3) {
+              for (int z = 2; z > pos; --z) { bs[z] = bs[z - 1]; bv[z] = bv[z - 1]; }
+              bs[pos] = s;
+              bv[pos] = vi;
+            }
+          }
+        } else {
+          if (sp >= kStack) { overflow = true; break; }
+          stack[sp++] = ch[side];
+        }
+      }
+      if (overflow) break;
+    }
+    if (overflow) { count_add(A.counters, C_ERR_STACK, 1); continue; }
+    int32_t cand[kKnnCap];
+    int nc = 0;
+    for (int q = 0; q < 3 && !overflow; ++q) {
+      if (bv[q] < 0) continue;
+      for (int32_t e = A.ine_off[bv[q]]; e < A.ine_off[bv[q] + 1]; ++e) {
+        if (nc >= kKnnCap) { overflow = true; break; }
+        cand[nc++] = A.ine[e];
+      }
+    }
+    if (overflow) { count_add(A.counters, C_ERR_CAPACITY, 1); continue; }
+    for (int a = 1; a < nc; ++a) {  // insertion sort, then unique
+      const int32_t v = cand[a];
+      int b = a - 1;
+      while (b >= 0 && cand[b] > v) { cand[b + 1] = cand[b]; --b; }
+      cand[b + 1] = v;
+    }
+    double m = kBig;
+    d3 proj = {0.0, 0.0, 0.0};
+    for (int a = 0; a < nc; ++a) {
+      if (a > 0 && cand[a] == cand[a - 1]) continue;
+      tri_step64(A.rec[cand[a]], p, m, proj, true);
+    }
+    double d = m;
+    if (fabs(d) > fabs(g.h)) d = g.h;
+    A.dist[lin] = d;
+    if (A.xp) {
+      A.xp[3 * lin] = proj.x;
+      A.xp[3 * lin + 1] = proj.y;
+      A.xp[3 * lin + 2] = proj.z;
+    }
+    ++done;
+  }
+  for (int off = 16; off > 0; off >>= 1) done += __shfl_down_sync(0xffffffffu, done, off);
+  if ((threadIdx.x & 31) == 0 && done) count_add(A.counters, C_KNN, done);
+}
+
+struct UnbArgs {
+  GridP g;
+  const BNode* nodes;
+  const int32_t* leaf_prim;
+  const float4* v32;
+  const TriRec64* rec;
+  float pad;
+  float eD_abs, eD_rel;
+  int64_t max_visits;
+  double* dist;
+  double* xp;
+  int64_t* counters;
+};
+
+// True nearest triangle (no clamp): depth-first LBVH search, nearer child first, FP32 bounds,
+// FP64 reference arithmetic for the candidates inside the FP32 error band.
+__global__ void __launch_bounds__(128) k_unbounded(UnbArgs A) {
+  const GridP& g = A.g;
+  int64_t fp64 = 0;
+  for (int64_t lin = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; lin < g.ngp; lin += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i, j, k;
+    node_ijk(g, lin, i, j, k);
+    const d3 p = node_coord(g.o, g.h, i, j, k);
+    const float3 p32 = local32(g, p);
+    double m = kBig;
+    d3 proj = {0.0, 0.0, 0.0};
+    bool have = false, overflow = false;
+    int stack[kStack];
+    int sp = 0;
+    stack[sp++] = 0;
+    int64_t visits = 0;
+    while (sp > 0) {
+      if (++visits > A.max_visits) { overflow = true; break; }
+      const BNode nd = A.nodes[stack[--sp]];
+      const float bound = have ? (float)m + A.eD_abs + A.eD_rel * (float)m + A.pad : INFINITY;
+      float3 lo0, hi0, lo1, hi1;
+      child_box(nd, 0, lo0, hi0);
+      child_box(nd, 1, lo1, hi1);
+      float d0 = lo0.x > hi0.x ? INFINITY : box_d2(p32, lo0, hi0);
+      float d1 = lo1.x > hi1.x ? INFINITY : box_d2(p32, lo1, hi1);
+      const float b2 = bound * bound;
+      int c0 = nd.d.x, c1 = nd.d.y;
+      if (d1 < d0) {  // visit the nearer child first: push it last
+        float t = d0; d0 = d1; d1 = t;
+        int c = c0; c0 = c1; c1 = c;
+      }
+      const int cs[2] = {c1, c0};
+      const float ds2[2] = {d1, d0};
+      for (int q = 0; q < 2; ++q) {
+        if (!(ds2[q] <= b2) && have) continue;
+        if (isinf(ds2[q])) continue;
+        if (cs[q] & kLeafBit) {
+          const int prim = A.leaf_prim[cs[q] & 0x7fffffff];
+          if (have) {
+            const float D = sqrtf(pt_tri_d2(p32, f3(A.v32[3 * prim]), f3(A.v32[3 * prim + 1]), f3(A.v32[3 * prim + 2])));
+            if ((double)D > m + (double)(A.eD_abs + A.eD_rel * (float)m)) continue;
+          }
+          tri_step64(A.rec[prim], p, m, proj, false);
+          have = true;
+          ++fp64;
+        } else {
+          if (sp >= kStack) { overflow = true; break; }
+          stack[sp++] = cs[q];
+        }
+      }
+      if (overflow) break;
+    }
+    if (overflow) count_add(A.counters, C_ERR_STACK, 1);
+    A.dist[lin] = m;
+    if (A.xp) {
+      A.xp[3 * lin] = proj.x;
+      A.xp[3 * lin + 1] = proj.y;
+      A.xp[3 * lin + 2] = proj.z;
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) fp64 += __shfl_down_sync(0xffffffffu, fp64, off);
+  if ((threadIdx.x & 31) == 0 && fp64) count_add(A.counters, C_FP64, fp64);
+}
+
+int ceil_log2(uint64_t v) {
+  int b = 0;
+  while ((1ULL << b) < v) ++b;
+  return b < 1 ? 1 : b;
+}
+
+}  // namespace
+
+int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, double* d_dist, double* d_xp) {
+  cudaStream_t st = ctx->stream;
+  const MeshDev& M = ctx->mesh;
+  const int64_t nel = M.nel;
+  TriRec64* rec = buf<TriRec64>(ctx, "rec");
+  double4* cent = buf<double4>(ctx, "cent64");
+  float4* v32 = buf<float4>(ctx, "v32");
+  float4* c32 = buf<float4>(ctx, "c32");
+  BNode* nodes = buf<BNode>(ctx, "nodes");
+  int32_t* leaf_prim = buf<int32_t>(ctx, "leaf_prim");
+  // FP32 error model: coordinates in the mesh-local frame are within E, so each FP32 coordinate
+  // carries at most 2^-24 E; the bounds below keep a >= 8x margin over the worst accumulation.
+  const float E = (float)g.E;
+  const float eD_abs = 4.0e-6f * E;
+  const float eD_rel = 4.0e-6f;
+  const float pad = 2.0e-6f * E;
+
+  if (mode == SDFGPU_MODE_UNBOUNDED) {
+    (void)use_learned;
+    UnbArgs A{g, nodes, leaf_prim, v32, rec, pad, eD_abs, eD_rel, 2 * nel + 64, d_dist, d_xp, ctx->d_counters};
+    k_unbounded<<<grid_for(g.ngp, 128, 148 * 32), 128, 0, st>>>(A);
+    SDF_CUDA(ctx, cudaGetLastError());
+    return 0;
+  }
+
+  const double sr = 2.5 * g.h;
+  const double R = mode == SDFGPU_MODE_REF_RULE ? sr * (1.0 + 1e-9) + 1e-6 * g.E : g.h * (1.0 + 1e-9) + 1e-6 * g.E;
+  int32_t *tri_cnt, *tri_off, *tile_cnt, *tile_off, *vals, *vals2;
+  uint32_t *keys, *keys2;
+  uint8_t* status;
+  SDF_TRY(scratch_t(ctx, "tri_cnt", (size_t)nel + 1, &tri_cnt));
+  SDF_TRY(scratch_t(ctx, "tri_off", (size_t)nel + 1, &tri_off));
+  SDF_TRY(scratch_t(ctx, "tile_cnt", (size_t)g.ntiles + 1, &tile_cnt));
+  SDF_TRY(scratch_t(ctx, "tile_off", (size_t)g.ntiles + 1, &tile_off));
+  SDF_TRY(scratch_t(ctx, "status", (size_t)g.ngp, &status));
+  SDF_CUDA(ctx, cudaMemsetAsync(tile_cnt, 0, sizeof(int32_t) * (g.ntiles + 1), st));
+  SDF_CUDA(ctx, cudaMemsetAsync(tri_cnt + nel, 0, sizeof(int32_t), st));
+  k_tile_pairs<false><<<grid_for(nel, 128), 128, 0, st>>>(cent, rec, nel, g, mode, R, tri_cnt, nullptr, tile_cnt,
+                                                          nullptr, nullptr);
+  SDF_CUDA(ctx, cudaGetLastError());
+  SDF_TRY(cub_scan_i32(ctx, tri_cnt, tri_off, nel + 1));
+  int32_t total = 0;
+  SDF_CUDA(ctx, cudaMemcpyAsync(&total, tri_off + nel, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  SDF_CUDA(ctx, cudaStreamSynchronize(st));
+  if (total < 0) return fail(ctx, SDFGPU_ERR_CAPACITY, "more than 2^31 (tile, triangle) pairs; use a coarser grid");
+  ctx->h_counters[C_TILE_PAIRS] = total;
+  const size_t P = (size_t)std::max<int32_t>(total, 1);
+  SDF_TRY(scratch_t(ctx, "pair_keys", P, &keys));
+  SDF_TRY(scratch_t(ctx, "pair_keys2", P, &keys2));
+  SDF_TRY(scratch_t(ctx, "pair_vals", P, &vals));
+  SDF_TRY(scratch_t(ctx, "pair_vals2", P, &vals2));
+  if (total > 0) {
+    k_tile_pairs<true><<<grid_for(nel, 128), 128, 0, st>>>(cent, rec, nel, g, mode, R, nullptr, tri_off, nullptr,
+                                                           keys, vals);
+    SDF_CUDA(ctx, cudaGetLastError());
+    const int bits = ceil_log2((uint64_t)g.ntiles + 1);
+    size_t tmp_bytes = 0;
+    SDF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys2, vals, vals2, total, 0, bits, st));
+    void* tmp;
+    SDF_TRY(scratch(ctx, "cub_tmp", tmp_bytes, &tmp));
+    SDF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys2, vals, vals2, total, 0, bits, st));
+  }
+  SDF_TRY(cub_scan_i32(ctx, tile_cnt, tile_off, g.ntiles + 1));
+
+  FoldArgs A;
+  A.g = g;
+  A.mode = mode;
+  A.tile_off = tile_off;
+  A.tile_cnt = tile_cnt;
+  A.vals = vals2;
+  A.rec = rec;
+  A.cent = cent;
+  A.v32 = v32;
+  A.c32 = c32;
+  A.r2 = sr * sr;
+  const double e_c = 1e-6 * (g.E + sr);
+  A.r2_in = (float)((sr - e_c) * (sr - e_c));
+  A.r2_out = (float)((sr + e_c) * (sr + e_c));
+  A.eD_abs = eD_abs;
+  A.eD_rel = eD_rel;
+  A.dist = d_dist;
+  A.xp = d_xp;
+  A.status = status;
+  A.counters = ctx->d_counters;
+  const int threads = g.t[0] * g.t[1] * g.t[2];
+  if (g.ntiles > 0x7fffffffLL) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "grid has too many tiles");
+  k_tile_fold<<<(unsigned)g.ntiles, threads, 0, st>>>(A);
+  SDF_CUDA(ctx, cudaGetLastError());
+
+  if (mode == SDFGPU_MODE_REF_RULE) {
+    // Can a node with an empty candidate set still have a triangle within h?  Only when some
+    // triangle reaches farther than 1.5h from its centroid (|c - p| <= d + rho <= h + rho).
+    const bool big_tris = M.rho_max * (1.0 + 1e-9) + 1e-6 * g.E >= 1.5 * g.h;
+    if (big_tris || d_xp) {
+      SDF_TRY(ensure_ine(ctx));
+      uint8_t* band = nullptr;
+      if (!d_xp) {
+        SDF_TRY(scratch_t(ctx, "band", (size_t)g.ngp, &band));
+        SDF_CUDA(ctx, cudaMemsetAsync(band, 0, (size_t)g.ngp, st));
+        const double hb = g.h * (1.0 + 1e-9) + (double)eD_abs + 2e-6 * g.E;
+        k_band<<<grid_for(nel, 128), 128, 0, st>>>(v32, rec, nel, g, hb, (float)(hb * hb), band);
+        SDF_CUDA(ctx, cudaGetLastError());
+      }
+      KnnArgs K;
+      K.g = g;
+      K.status = status;
+      K.band = band;
+      K.nodes = nodes;
+      K.leaf_prim = leaf_prim;
+      K.tri_idx = nullptr;
+      K.IEN = buf<int64_t>(ctx, "IEN64");
+      K.X = buf<double>(ctx, "X64");
+      K.ine_off = buf<int32_t>(ctx, "ine_off");
+      K.ine = buf<int32_t>(ctx, "ine");
+      K.rec = rec;
+      K.pad = pad;
+      K.max_visits = 2 * nel + 64;
+      K.dist = d_dist;
+      K.xp = d_xp;
+      K.counters = ctx->d_counters;
+      k_knn_fallback<<<grid_for(g.ngp, 128, 148 * 16), 128, 0, st>>>(K);
+      SDF_CUDA(ctx, cudaGetLastError());
+    }
+  }
+  return 0;
+}
+
+}  // namespace sdfgpu

@@ -1,0 +1,78 @@
+// geom32.cuh -- FP32 geometry for the bulk of the work: point-triangle distance and ray-box
+// tests in mesh-local coordinates (vertices minus the mesh's bounding-box centre).  Every FP32
+// result is used only as a filter with an explicit error margin; decisions that land inside the
+// margin are re-made with the FP64 routines of exact64.cuh.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace sdfgpu {
+
+__device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float dot3f(float3 a, float3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
+__device__ __forceinline__ float3 cross3f(float3 a, float3 b) {
+  return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+// Squared distance from p to segment [a, a+e].
+__device__ __forceinline__ float seg_d2(float3 p, float3 a, float3 e) {
+  const float3 w = p - a;
+  const float ee = dot3f(e, e);
+  float t = ee > 0.f ? dot3f(w, e) / ee : 0.f;
+  t = fminf(fmaxf(t, 0.f), 1.f);
+  const float3 q = w - e * t;
+  return dot3f(q, q);
+}
+
+// Squared distance from p to triangle (a, b, c): minimum of the three edge distances and, when
+// p projects inside, the plane distance.  Degenerate triangles reduce to their edges.
+__device__ __forceinline__ float pt_tri_d2(float3 p, float3 a, float3 b, float3 c) {
+  const float3 ab = b - a, bc = c - b, ca = a - c;
+  float d2 = fminf(seg_d2(p, a, ab), fminf(seg_d2(p, b, bc), seg_d2(p, c, ca)));
+  const float3 n = cross3f(ab, c - a);
+  const float nn = dot3f(n, n);
+  if (nn > 0.f) {
+    const float s1 = dot3f(cross3f(ab, p - a), n);
+    const float s2 = dot3f(cross3f(bc, p - b), n);
+    const float s3 = dot3f(cross3f(ca, p - c), n);
+    if (s1 >= 0.f && s2 >= 0.f && s3 >= 0.f) {
+      const float pd = dot3f(p - a, n);
+      d2 = fminf(d2, pd * pd / nn);
+    }
+  }
+  return d2;
+}
+
+// Squared distance from p to the box [lo, hi].
+__device__ __forceinline__ float box_d2(float3 p, float3 lo, float3 hi) {
+  const float dx = fmaxf(fmaxf(lo.x - p.x, p.x - hi.x), 0.f);
+  const float dy = fmaxf(fmaxf(lo.y - p.y, p.y - hi.y), 0.f);
+  const float dz = fmaxf(fmaxf(lo.z - p.z, p.z - hi.z), 0.f);
+  return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+}
+
+// Slab test of the half-line o + t d (t >= -tpad) against [lo - pad, hi + pad].  inv holds
+// 1/d per axis (inf where d is 0; such axes test containment of o instead).
+__device__ __forceinline__ bool ray_box(float3 o, float3 d, float3 inv, float3 lo, float3 hi, float pad,
+                                        float tpad) {
+  float t0 = -tpad, t1 = 3.0e38f;
+  if (d.x != 0.f) {
+    float a = (lo.x - pad - o.x) * inv.x, b = (hi.x + pad - o.x) * inv.x;
+    t0 = fmaxf(t0, fminf(a, b)); t1 = fminf(t1, fmaxf(a, b));
+  } else if (o.x < lo.x - pad || o.x > hi.x + pad) return false;
+  if (d.y != 0.f) {
+    float a = (lo.y - pad - o.y) * inv.y, b = (hi.y + pad - o.y) * inv.y;
+    t0 = fmaxf(t0, fminf(a, b)); t1 = fminf(t1, fmaxf(a, b));
+  } else if (o.y < lo.y - pad || o.y > hi.y + pad) return false;
+  if (d.z != 0.f) {
+    float a = (lo.z - pad - o.z) * inv.z, b = (hi.z + pad - o.z) * inv.z;
+    t0 = fmaxf(t0, fminf(a, b)); t1 = fminf(t1, fmaxf(a, b));
+  } else if (o.z < lo.z - pad || o.z > hi.z + pad) return false;
+  return t0 <= t1 + tpad;
+}
+
+}  // namespace sdfgpu

@@ -1,0 +1,376 @@
+// mesh.cu -- TriangularMesh upload, per-triangle preparation and the LBVH build.
+//
+// Reference: TriangularMesh (src/MeshGrid/MeshInformations.jl:57-84), prepare_triangle_data
+// (src/SignedDistances/dfOnTriangularMesh.jl:329-368) and the two acceleration structures the
+// reference builds per call (KD-trees at dfOnTriangularMesh.jl:27,35; ImplicitBVH at
+// RaycastingSignDetection.jl:35-56).  Here one LBVH over triangle boxes serves every query that
+// is not grid-structured: arbitrary-direction rays, the 3-nearest-vertex fallback and the
+// unbounded nearest-triangle search.
+//
+// LBVH (Karras 2012, "Maximizing parallelism in the construction of BVHs, octrees, and k-d
+// trees"): 30-bit Morton codes of the triangle centroids with the triangle index in the low 32
+// bits (unique 64-bit keys), a CUB radix sort, one thread per internal node to find its range
+// and split, then a bottom-up refit with one atomic counter per internal node.
+#include <cub/cub.cuh>
+
+#include "common.cuh"
+
+namespace sdfgpu {
+
+namespace {
+
+__global__ void k_vertex_bbox(const double* __restrict__ X, int64_t nnp, unsigned long long* bb) {
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  bool nonfinite = false;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nnp; v += (int64_t)gridDim.x * blockDim.x) {
+    for (int a = 0; a < 3; ++a) {
+      const double x = X[3 * v + a];
+      if (!isfinite(x)) nonfinite = true;
+      lo[a] = fmin(lo[a], x);
+      hi[a] = fmax(hi[a], x);
+    }
+  }
+  for (int a = 0; a < 3; ++a) {
+    for (int off = 16; off > 0; off >>= 1) {
+      lo[a] = fmin(lo[a], __shfl_down_sync(0xffffffffu, lo[a], off));
+      hi[a] = fmax(hi[a], __shfl_down_sync(0xffffffffu, hi[a], off));
+    }
+  }
+  const unsigned nf = __ballot_sync(0xffffffffu, nonfinite);
+  if ((threadIdx.x & 31) == 0) {
+    for (int a = 0; a < 3; ++a) {
+      atomicMin(&bb[a], dbl_ord(lo[a]));
+      atomicMax(&bb[3 + a], dbl_ord(hi[a]));
+    }
+    if (nf) atomicOr(&bb[6], 1ULL);
+  }
+}
+
+// Per-triangle FP64 record (dfOnTriangularMesh.jl:329-368) and the barycentric factorization.
+__global__ void k_prep(const double* __restrict__ X, int64_t nnp, const int64_t* __restrict__ IEN, int64_t nel,
+                       TriRec64* __restrict__ rec, double4* __restrict__ cent, int64_t* counters) {
+  for (int64_t el = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; el < nel; el += (int64_t)gridDim.x * blockDim.x) {
+    TriRec64 r;
+    d3 v[3];
+    for (int k = 0; k < 3; ++k) {
+      int64_t vi = IEN[3 * el + k];
+      if (vi < 1 || vi > nnp) {
+        count_add(counters, C_ERR_INDEX, 1);
+        vi = 1;
+      }
+      vi -= 1;
+      v[k] = {X[3 * vi], X[3 * vi + 1], X[3 * vi + 2]};
+      r.v[3 * k] = v[k].x; r.v[3 * k + 1] = v[k].y; r.v[3 * k + 2] = v[k].z;
+    }
+    const d3 e[3] = {v_sub(v[1], v[0]), v_sub(v[2], v[1]), v_sub(v[0], v[2])};
+    for (int j = 0; j < 3; ++j) {
+      r.L[j] = v_norm(e[j]);
+      const d3 u = v_div(e[j], r.L[j]);
+      r.u[3 * j] = u.x; r.u[3 * j + 1] = u.y; r.u[3 * j + 2] = u.z;
+    }
+    const d3 nn = v_cross(e[0], v_neg(e[2]));
+    const d3 n = v_div(nn, v_norm(nn));
+    r.n[0] = n.x; r.n[1] = n.y; r.n[2] = n.z;
+    const d3 c = v_div(v_add(v_add(v[0], v[1]), v[2]), 3.0);
+    r.bmin[0] = fmin(v[0].x, fmin(v[1].x, v[2].x));
+    r.bmin[1] = fmin(v[0].y, fmin(v[1].y, v[2].y));
+    r.bmin[2] = fmin(v[0].z, fmin(v[1].z, v[2].z));
+    r.bmax[0] = fmax(v[0].x, fmax(v[1].x, v[2].x));
+    r.bmax[1] = fmax(v[0].y, fmax(v[1].y, v[2].y));
+    r.bmax[2] = fmax(v[0].z, fmax(v[1].z, v[2].z));
+    r.pad = 0;
+    factor_bary(r);
+    rec[el] = r;
+    cent[el] = make_double4(c.x, c.y, c.z, 0.0);
+  }
+}
+
+// Mesh-local FP32 copies: vertices, centroid, outward-rounded box; and rho = max vertex
+// distance from the centroid (decides whether the centroid rule can miss a triangle within h).
+__global__ void k_local32(const TriRec64* __restrict__ rec, const double4* __restrict__ cent, int64_t nel, double cx,
+                          double cy, double cz, float4* __restrict__ v32, float4* __restrict__ c32,
+                          float4* __restrict__ box32, unsigned long long* rho_ord) {
+  double rho = 0.0;
+  for (int64_t el = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; el < nel; el += (int64_t)gridDim.x * blockDim.x) {
+    const TriRec64& r = rec[el];
+    const double4 c = cent[el];
+    for (int k = 0; k < 3; ++k) {
+      const double x = r.v[3 * k], y = r.v[3 * k + 1], z = r.v[3 * k + 2];
+      v32[3 * el + k] = make_float4((float)(x - cx), (float)(y - cy), (float)(z - cz), 0.f);
+      const double dx = x - c.x, dy = y - c.y, dz = z - c.z;
+      rho = fmax(rho, sqrt(dx * dx + dy * dy + dz * dz));
+    }
+    c32[el] = make_float4((float)(c.x - cx), (float)(c.y - cy), (float)(c.z - cz), 0.f);
+    box32[2 * el] = make_float4(__double2float_rd(r.bmin[0] - cx), __double2float_rd(r.bmin[1] - cy),
+                                __double2float_rd(r.bmin[2] - cz), 0.f);
+    box32[2 * el + 1] = make_float4(__double2float_ru(r.bmax[0] - cx), __double2float_ru(r.bmax[1] - cy),
+                                    __double2float_ru(r.bmax[2] - cz), 0.f);
+  }
+  for (int off = 16; off > 0; off >>= 1) rho = fmax(rho, __shfl_down_sync(0xffffffffu, rho, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(rho_ord, dbl_ord(rho * (1.0 + 1e-12)));
+}
+
+__device__ __forceinline__ unsigned expand_bits10(unsigned v) {
+  v = (v * 0x00010001u) & 0xFF0000FFu;
+  v = (v * 0x00000101u) & 0x0F00F00Fu;
+  v = (v * 0x00000011u) & 0xC30C30C3u;
+  v = (v * 0x00000005u) & 0x49249249u;
+  return v;
+}
+
+__global__ void k_morton(const float4* __restrict__ c32, int64_t nel, float lox, float loy, float loz, float inv,
+                         unsigned long long* __restrict__ keys) {
+  for (int64_t el = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; el < nel; el += (int64_t)gridDim.x * blockDim.x) {
+    const float4 c = c32[el];
+    const float fx = fminf(fmaxf((c.x - lox) * inv, 0.f), 1023.f);
+    const float fy = fminf(fmaxf((c.y - loy) * inv, 0.f), 1023.f);
+    const float fz = fminf(fmaxf((c.z - loz) * inv, 0.f), 1023.f);
+    const unsigned m = (expand_bits10((unsigned)fx) << 2) | (expand_bits10((unsigned)fy) << 1) | expand_bits10((unsigned)fz);
+    keys[el] = ((unsigned long long)m << 32) | (unsigned long long)el;
+  }
+}
+
+__device__ __forceinline__ int kdelta(const unsigned long long* __restrict__ k, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  return __clzll(k[i] ^ k[j]);
+}
+
+__global__ void k_karras(const unsigned long long* __restrict__ keys, int n, BNode* __restrict__ nodes,
+                         int32_t* __restrict__ int_parent, int32_t* __restrict__ leaf_parent) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1; i += gridDim.x * blockDim.x) {
+    const int d = (kdelta(keys, n, i, i + 1) - kdelta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    const int dmin = kdelta(keys, n, i, i - d);
+    int lmax = 2;
+    while (kdelta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+      if (kdelta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    const int j = i + l * d;
+    const int dnode = kdelta(keys, n, i, j);
+    int s = 0, t = l;
+    while (true) {
+      t = (t + 1) >> 1;
+      if (kdelta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+      if (t <= 1) break;
+    }
+    const int gamma = i + s * d + (d < 0 ? -1 : 0);
+    const int lo = min(i, j), hi = max(i, j);
+    int left, right;
+    if (lo == gamma) { left = kLeafBit | gamma; leaf_parent[gamma] = i; }
+    else { left = gamma; int_parent[gamma] = i; }
+    if (hi == gamma + 1) { right = kLeafBit | (gamma + 1); leaf_parent[gamma + 1] = i; }
+    else { right = gamma + 1; int_parent[gamma + 1] = i; }
+    nodes[i].d = make_int4(left, right, 0, 0);
+  }
+}
+
+__global__ void k_refit(const unsigned long long* __restrict__ keys, const float4* __restrict__ box32, int n,
+                        BNode* nodes, const int32_t* __restrict__ int_parent, const int32_t* __restrict__ leaf_parent,
+                        int32_t* flags, int32_t* __restrict__ leaf_prim) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int prim = (int)(keys[i] & 0xffffffffULL);
+    leaf_prim[i] = prim;
+    float4 lo = box32[2 * prim], hi = box32[2 * prim + 1];
+    int child = kLeafBit | i;
+    int node = leaf_parent[i];
+    int guard = 0;
+    while (node >= 0 && ++guard <= 128) {  // LBVH depth <= 64 for unique 64-bit keys
+      float* f = reinterpret_cast<float*>(&nodes[node]);
+      const int left = __ldcg(reinterpret_cast<const int*>(&nodes[node].d.x));
+      const int slot = (left == child) ? 0 : 6;
+      __stcg(f + slot + 0, lo.x); __stcg(f + slot + 1, lo.y); __stcg(f + slot + 2, lo.z);
+      __stcg(f + slot + 3, hi.x); __stcg(f + slot + 4, hi.y); __stcg(f + slot + 5, hi.z);
+      __threadfence();
+      if (atomicAdd(&flags[node], 1) == 0) break;
+      __threadfence();
+      float b[12];
+      for (int q = 0; q < 12; ++q) b[q] = __ldcg(f + q);
+      lo = make_float4(fminf(b[0], b[6]), fminf(b[1], b[7]), fminf(b[2], b[8]), 0.f);
+      hi = make_float4(fmaxf(b[3], b[9]), fmaxf(b[4], b[10]), fmaxf(b[5], b[11]), 0.f);
+      child = node;
+      node = int_parent[node];
+    }
+  }
+}
+
+// A single-triangle mesh: root with the leaf on the left and an empty box on the right.
+__global__ void k_single_root(const float4* __restrict__ box32, BNode* nodes, int32_t* leaf_prim) {
+  const float4 lo = box32[0], hi = box32[1];
+  BNode nd;
+  nd.a = make_float4(lo.x, lo.y, lo.z, hi.x);
+  nd.b = make_float4(hi.y, hi.z, 3.0e38f, 3.0e38f);
+  nd.c = make_float4(3.0e38f, -3.0e38f, -3.0e38f, -3.0e38f);
+  nd.d = make_int4(kLeafBit | 0, kLeafBit | 0, -1, 0);
+  nodes[0] = nd;
+  leaf_prim[0] = 0;
+}
+
+__global__ void k_ine_count(const int64_t* __restrict__ IEN, int64_t nel, int32_t* __restrict__ cnt) {
+  for (int64_t el = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; el < nel; el += (int64_t)gridDim.x * blockDim.x)
+    for (int k = 0; k < 3; ++k) atomicAdd(&cnt[IEN[3 * el + k] - 1], 1);
+}
+
+__global__ void k_ine_fill(const int64_t* __restrict__ IEN, int64_t nel, const int32_t* __restrict__ off,
+                           int32_t* __restrict__ cur, int32_t* __restrict__ ine) {
+  for (int64_t el = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; el < nel; el += (int64_t)gridDim.x * blockDim.x)
+    for (int k = 0; k < 3; ++k) {
+      const int64_t v = IEN[3 * el + k] - 1;
+      ine[off[v] + atomicAdd(&cur[v], 1)] = (int32_t)el;
+    }
+}
+
+}  // namespace
+
+int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const int64_t* IEN, int64_t nel,
+                          bool device_ptrs) {
+  cudaStream_t st = ctx->stream;
+  if (nel < 1 || nnp < 3) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "mesh needs at least 1 triangle and 3 vertices");
+  if (nel > (int64_t)0x7fffffff / 4) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "too many triangles (limit 536870911)");
+  if (!X || !IEN) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "X and IEN must not be NULL");
+  ctx->has_mesh = false;
+  ctx->mesh.ine_ready = false;
+  SDF_CUDA(ctx, cudaEventRecord(ctx->ev[4], st));
+
+  double* dX;
+  int64_t* dIEN;
+  SDF_TRY(scratch_t(ctx, "X64", (size_t)nnp * 3, &dX));
+  SDF_TRY(scratch_t(ctx, "IEN64", (size_t)nel * 3, &dIEN));
+  const cudaMemcpyKind kind = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  SDF_CUDA(ctx, cudaMemcpyAsync(dX, X, sizeof(double) * 3 * nnp, kind, st));
+  SDF_CUDA(ctx, cudaMemcpyAsync(dIEN, IEN, sizeof(int64_t) * 3 * nel, kind, st));
+
+  TriRec64* rec;
+  double4* cent;
+  float4 *v32, *c32, *box32;
+  unsigned long long* bb;
+  SDF_TRY(scratch_t(ctx, "rec", (size_t)nel, &rec));
+  SDF_TRY(scratch_t(ctx, "cent64", (size_t)nel, &cent));
+  SDF_TRY(scratch_t(ctx, "v32", (size_t)nel * 3, &v32));
+  SDF_TRY(scratch_t(ctx, "c32", (size_t)nel, &c32));
+  SDF_TRY(scratch_t(ctx, "box32", (size_t)nel * 2, &box32));
+  SDF_TRY(scratch_t(ctx, "bbox", 8, &bb));
+
+  unsigned long long init[8];
+  for (int a = 0; a < 3; ++a) { init[a] = ~0ULL; init[3 + a] = 0ULL; }
+  init[6] = 0ULL;
+  init[7] = 0ULL;  // rho (ordered encoding of 0.0 is > 0; reset below)
+  SDF_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, sizeof(int64_t) * C_NUM, st));
+  SDF_CUDA(ctx, cudaMemcpyAsync(bb, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  k_vertex_bbox<<<grid_for(nnp, 256, 148 * 8), 256, 0, st>>>(dX, nnp, bb);
+  SDF_CUDA(ctx, cudaGetLastError());
+  k_prep<<<grid_for(nel, 128), 128, 0, st>>>(dX, nnp, dIEN, nel, rec, cent, ctx->d_counters);
+  SDF_CUDA(ctx, cudaGetLastError());
+  unsigned long long hbb[8];
+  int64_t hcnt[C_NUM];
+  SDF_CUDA(ctx, cudaMemcpyAsync(hbb, bb, sizeof(hbb), cudaMemcpyDeviceToHost, st));
+  SDF_CUDA(ctx, cudaMemcpyAsync(hcnt, ctx->d_counters, sizeof(hcnt), cudaMemcpyDeviceToHost, st));
+  SDF_CUDA(ctx, cudaStreamSynchronize(st));
+  if (hbb[6]) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "mesh vertices must be finite");
+  if (hcnt[C_ERR_INDEX]) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "IEN holds an index outside 1..nnp");
+
+  MeshDev& M = ctx->mesh;
+  M.nnp = nnp;
+  M.nel = nel;
+  double E = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    M.bmin[a] = ord_dbl(hbb[a]);
+    M.bmax[a] = ord_dbl(hbb[3 + a]);
+    M.center[a] = 0.5 * (M.bmin[a] + M.bmax[a]);
+    E = std::max(E, std::max(M.bmax[a] - M.center[a], M.center[a] - M.bmin[a]));
+  }
+  M.E = E;
+
+  unsigned long long rho0 = 0ULL;  // below the encoding of every non-negative double
+  SDF_CUDA(ctx, cudaMemcpyAsync(bb + 7, &rho0, sizeof(rho0), cudaMemcpyHostToDevice, st));
+  k_local32<<<grid_for(nel, 128), 128, 0, st>>>(rec, cent, nel, M.center[0], M.center[1], M.center[2], v32, c32,
+                                                 box32, bb + 7);
+  SDF_CUDA(ctx, cudaGetLastError());
+
+  // LBVH
+  const int n = (int)nel;
+  unsigned long long *keys, *keys2;
+  BNode* nodes;
+  int32_t *int_parent, *leaf_parent, *flags, *leaf_prim;
+  SDF_TRY(scratch_t(ctx, "keys", (size_t)n, &keys));
+  SDF_TRY(scratch_t(ctx, "keys2", (size_t)n, &keys2));
+  SDF_TRY(scratch_t(ctx, "nodes", (size_t)std::max(1, n - 1), &nodes));
+  SDF_TRY(scratch_t(ctx, "int_parent", (size_t)n, &int_parent));
+  SDF_TRY(scratch_t(ctx, "leaf_parent", (size_t)n, &leaf_parent));
+  SDF_TRY(scratch_t(ctx, "flags", (size_t)n, &flags));
+  SDF_TRY(scratch_t(ctx, "leaf_prim", (size_t)n, &leaf_prim));
+  if (n == 1) {
+    k_single_root<<<1, 1, 0, st>>>(box32, nodes, leaf_prim);
+    SDF_CUDA(ctx, cudaGetLastError());
+  } else {
+    const float lox = (float)(M.bmin[0] - M.center[0]), loy = (float)(M.bmin[1] - M.center[1]),
+                loz = (float)(M.bmin[2] - M.center[2]);
+    const double ext = std::max(M.bmax[0] - M.bmin[0], std::max(M.bmax[1] - M.bmin[1], M.bmax[2] - M.bmin[2]));
+    const float inv = ext > 0 ? (float)(1024.0 / ext) : 1.0f;
+    k_morton<<<grid_for(nel, 256), 256, 0, st>>>(c32, nel, lox, loy, loz, inv, keys);
+    SDF_CUDA(ctx, cudaGetLastError());
+    size_t tmp_bytes = 0;
+    SDF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, keys, keys2, n, 0, 62, st));
+    void* tmp;
+    SDF_TRY(scratch(ctx, "cub_tmp", tmp_bytes, &tmp));
+    SDF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, keys, keys2, n, 0, 62, st));
+    SDF_CUDA(ctx, cudaMemsetAsync(int_parent, 0xff, sizeof(int32_t) * n, st));
+    SDF_CUDA(ctx, cudaMemsetAsync(flags, 0, sizeof(int32_t) * n, st));
+    k_karras<<<grid_for(n - 1, 256), 256, 0, st>>>(keys2, n, nodes, int_parent, leaf_parent);
+    SDF_CUDA(ctx, cudaGetLastError());
+    k_refit<<<grid_for(n, 256), 256, 0, st>>>(keys2, box32, n, nodes, int_parent, leaf_parent, flags, leaf_prim);
+    SDF_CUDA(ctx, cudaGetLastError());
+  }
+  unsigned long long hrho = 0;
+  SDF_CUDA(ctx, cudaMemcpyAsync(&hrho, bb + 7, sizeof(hrho), cudaMemcpyDeviceToHost, st));
+  SDF_CUDA(ctx, cudaEventRecord(ctx->ev[5], st));
+  SDF_CUDA(ctx, cudaStreamSynchronize(st));
+  M.rho_max = ord_dbl(hrho);
+  float ms = 0.f;
+  SDF_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]));
+  ctx->stats.ms_mesh = ms;
+  ctx->stats.nel = nel;
+  ctx->stats.rho_max = M.rho_max;
+  ctx->has_mesh = true;
+  return 0;
+}
+
+int ensure_ine(sdfgpu_ctx* ctx) {
+  MeshDev& M = ctx->mesh;
+  if (M.ine_ready) return 0;
+  cudaStream_t st = ctx->stream;
+  int32_t *cnt, *off, *cur, *ine;
+  SDF_TRY(scratch_t(ctx, "ine_cnt", (size_t)M.nnp + 1, &cnt));
+  SDF_TRY(scratch_t(ctx, "ine_off", (size_t)M.nnp + 1, &off));
+  SDF_TRY(scratch_t(ctx, "ine_cur", (size_t)M.nnp + 1, &cur));
+  SDF_TRY(scratch_t(ctx, "ine", (size_t)M.nel * 3, &ine));
+  const int64_t* dIEN = buf<int64_t>(ctx, "IEN64");
+  SDF_CUDA(ctx, cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (M.nnp + 1), st));
+  SDF_CUDA(ctx, cudaMemsetAsync(cur, 0, sizeof(int32_t) * (M.nnp + 1), st));
+  k_ine_count<<<grid_for(M.nel, 256), 256, 0, st>>>(dIEN, M.nel, cnt);
+  SDF_CUDA(ctx, cudaGetLastError());
+  SDF_TRY(cub_scan_i32(ctx, cnt, off, M.nnp + 1));
+  k_ine_fill<<<grid_for(M.nel, 256), 256, 0, st>>>(dIEN, M.nel, off, cur, ine);
+  SDF_CUDA(ctx, cudaGetLastError());
+  M.ine_ready = true;
+  return 0;
+}
+
+int cub_scan_i32(sdfgpu_ctx* ctx, const int32_t* in, int32_t* out, int64_t n) {
+  size_t bytes = 0;
+  SDF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, (int)n, ctx->stream));
+  void* tmp;
+  SDF_TRY(scratch(ctx, "cub_tmp_scan", bytes, &tmp));
+  SDF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, (int)n, ctx->stream));
+  return 0;
+}
+
+int cub_scan_i64(sdfgpu_ctx* ctx, const int64_t* in, int64_t* out, int64_t n) {
+  size_t bytes = 0;
+  SDF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, (int)n, ctx->stream));
+  void* tmp;
+  SDF_TRY(scratch(ctx, "cub_tmp_scan", bytes, &tmp));
+  SDF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, (int)n, ctx->stream));
+  return 0;
+}
+
+}  // namespace sdfgpu

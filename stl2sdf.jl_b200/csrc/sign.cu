@@ -1,0 +1,562 @@
+// sign.cu -- raycast_sign_detection (src/SignedDistances/RaycastingSignDetection.jl:337-404).
+//
+// Per node the reference casts the prioritized directions (:162-227) and votes by the parity of
+// the distinct Möller–Trumbore hits (:114-154): 6 axis rays, then batches of 4 until the vote
+// is confident (:234-288), then the generalized winding number when confidence < 0.6 (:376-380).
+//
+// B200 layout of the work:
+//   * The 6 axis rays are the only rays every node casts, and they are grid-structured.  For a
+//     ray along +x from node (i, j, k) every Möller–Trumbore decision except t > eps depends only
+//     on the row (j, k): h = cross(e_x, e2) has an exactly zero x component, so u and v never see
+//     the node's x.  And the -x ray of the same node sees a = -a, f = -f, the same u and v, and
+//     t = -t exactly.  So one list of (row, triangle) hits per axis serves both directions of
+//     every node of the row.  The lists are built by a triangle scatter over the rows its
+//     projected box covers (FP64 decisions, exactly the reference's); each node then evaluates
+//     only t for the hits of its three rows with the reference's formula, sorts, de-duplicates
+//     within eps and takes parities.  A warp walks 32 consecutive nodes of one row, so the row's
+//     hits are broadcast loads.
+//   * Nodes whose 6 votes disagree continue with the reference's batches on the LBVH: FP32 slab
+//     tests with an explicit margin prune, FP64 Möller–Trumbore decides.
+//   * Nodes left with confidence < threshold sum the winding number over all triangles, one CTA
+//     per node with a fixed-order block reduction.
+#include <cub/cub.cuh>
+
+#include "common.cuh"
+
+namespace sdfgpu {
+
+__constant__ double c_dirs[36 * 3];
+
+namespace {
+
+constexpr double kEps = 1e-8;  // check_ray_inside_bvh default (:118), passed to MT (:132)
+constexpr int kRowCap = 64;    // hits per row a node sorts in registers/local memory
+constexpr int kRayCap = 256;   // hits per generic ray
+constexpr int kStack = 64;
+
+// A row hit: the Möller–Trumbore constants of one triangle for one grid row, from which each node
+// of the row gets t with the reference's operation order (see the per-axis formulas below).
+struct __align__(16) RowHit {
+  double v1a;  // v1 coordinate along the row axis
+  double K1, K2, P;
+  double ea, eb, fa, fb;
+  double f;
+  double key;  // approximate hit coordinate along the axis (row ordering only)
+};
+
+template <int AX>
+__device__ __forceinline__ double row_t(const RowHit& r, double xa) {
+  const double s = ds(xa, r.v1a);
+  if (AX == 0) {
+    const double qy = ds(r.K1, dm(s, r.ea));
+    const double qz = ds(dm(s, r.eb), r.K2);
+    return dm(r.f, da(da(r.P, dm(r.fa, qy)), dm(r.fb, qz)));
+  } else if (AX == 1) {
+    const double qx = ds(dm(s, r.ea), r.K1);
+    const double qz = ds(r.K2, dm(s, r.eb));
+    return dm(r.f, da(da(dm(r.fa, qx), r.P), dm(r.fb, qz)));
+  } else {
+    const double qx = ds(r.K1, dm(s, r.ea));
+    const double qy = ds(dm(s, r.eb), r.K2);
+    return dm(r.f, da(da(dm(r.fa, qx), dm(r.fb, qy)), r.P));
+  }
+}
+
+// Möller–Trumbore decisions of the +AX ray through (ob, oc) against the triangle; on a pass fills
+// the row-hit constants.  The along-axis origin is v1's own coordinate (any value gives the same
+// decisions, see the file comment).
+template <int AX>
+__device__ __forceinline__ bool row_test(const TriRec64& r, double ob, double oc, RowHit* out) {
+  const d3 v1 = rec_v(r, 0), v2 = rec_v(r, 1), v3 = rec_v(r, 2);
+  d3 o, d;
+  if (AX == 0) { o = {v1.x, ob, oc}; d = {1.0, 0.0, 0.0}; }
+  else if (AX == 1) { o = {ob, v1.y, oc}; d = {0.0, 1.0, 0.0}; }
+  else { o = {ob, oc, v1.z}; d = {0.0, 0.0, 1.0}; }
+  const d3 e1 = v_sub(v2, v1), e2 = v_sub(v3, v1);
+  const d3 h = v_cross(d, e2);
+  const double a = v_dot(e1, h);
+  if (fabs(a) < kEps) return false;
+  const double f = dd(1.0, a);
+  const d3 s = v_sub(o, v1);
+  const double u = dm(f, v_dot(s, h));
+  if (u < 0.0 || u > 1.0) return false;
+  const d3 q = v_cross(s, e1);
+  const double v = dm(f, v_dot(d, q));
+  if (v < 0.0 || da(u, v) > 1.0) return false;
+  if (out) {
+    RowHit R;
+    R.f = f;
+    if (AX == 0) {
+      R.v1a = v1.x; R.K1 = dm(s.z, e1.x); R.K2 = dm(s.y, e1.x); R.P = dm(e2.x, q.x);
+      R.ea = e1.z; R.eb = e1.y; R.fa = e2.y; R.fb = e2.z;
+    } else if (AX == 1) {
+      R.v1a = v1.y; R.K1 = dm(s.z, e1.y); R.K2 = dm(s.x, e1.y); R.P = dm(e2.y, q.y);
+      R.ea = e1.z; R.eb = e1.x; R.fa = e2.x; R.fb = e2.z;
+    } else {
+      R.v1a = v1.z; R.K1 = dm(s.y, e1.z); R.K2 = dm(s.x, e1.z); R.P = dm(e2.z, q.z);
+      R.ea = e1.y; R.eb = e1.x; R.fa = e2.x; R.fb = e2.y;
+    }
+    R.key = R.v1a + row_t<AX>(R, R.v1a);
+    *out = R;
+  }
+  return true;
+}
+
+__device__ __forceinline__ bool axis_range2(const GridP& g, int a, double x0, double x1, int64_t& lo, int64_t& hi) {
+  double f0 = (x0 - g.o[a]) / g.h - 1e-6, f1 = (x1 - g.o[a]) / g.h + 1e-6;
+  f0 = fmax(f0, -1.0);
+  f1 = fmin(f1, (double)g.N[a] + 1.0);
+  if (!(f0 <= f1)) return false;
+  lo = (int64_t)ceil(f0);
+  hi = (int64_t)floor(f1);
+  if (lo < 0) lo = 0;
+  if (hi > g.N[a]) hi = g.N[a];
+  return lo <= hi;
+}
+
+template <int AX>
+__device__ __forceinline__ void tri_rows(const GridP& g, const TriRec64& r, bool fill, int64_t row_base,
+                                         int32_t* row_cnt, const int32_t* row_off, int32_t* row_cur, RowHit* hits,
+                                         int64_t& nhit) {
+  const int b = AX == 0 ? 1 : 0, c = AX == 2 ? 1 : 2;
+  int64_t b0, b1, c0, c1;
+  if (!axis_range2(g, b, r.bmin[b], r.bmax[b], b0, b1)) return;
+  if (!axis_range2(g, c, r.bmin[c], r.bmax[c], c0, c1)) return;
+  for (int64_t jc = c0; jc <= c1; ++jc) {
+    const double oc = da(g.o[c], dm(g.h, (double)jc));
+    for (int64_t jb = b0; jb <= b1; ++jb) {
+      const double ob = da(g.o[b], dm(g.h, (double)jb));
+      const int64_t row = row_base + jc * g.n[b] + jb;
+      if (!fill) {
+        if (row_test<AX>(r, ob, oc, nullptr)) { atomicAdd(&row_cnt[row], 1); ++nhit; }
+      } else {
+        RowHit R;
+        if (row_test<AX>(r, ob, oc, &R)) {
+          const int32_t slot = atomicAdd(&row_cur[row], 1);
+          hits[row_off[row] + slot] = R;
+        }
+      }
+    }
+  }
+}
+
+__global__ void k_rows(const TriRec64* __restrict__ rec, int64_t nel, GridP g, int64_t base_y, int64_t base_z,
+                       bool fill, int32_t* row_cnt, const int32_t* row_off, int32_t* row_cur, RowHit* hits,
+                       int64_t* counters) {
+  int64_t nhit = 0;
+  for (int64_t el = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; el < nel; el += (int64_t)gridDim.x * blockDim.x) {
+    const TriRec64 r = rec[el];
+    tri_rows<0>(g, r, fill, 0, row_cnt, row_off, row_cur, hits, nhit);
+    tri_rows<1>(g, r, fill, base_y, row_cnt, row_off, row_cur, hits, nhit);
+    tri_rows<2>(g, r, fill, base_z, row_cnt, row_off, row_cur, hits, nhit);
+  }
+  if (!fill) {
+    for (int off = 16; off > 0; off >>= 1) nhit += __shfl_down_sync(0xffffffffu, nhit, off);
+    if ((threadIdx.x & 31) == 0 && nhit) count_add(counters, C_ROW_HITS, nhit);
+  }
+}
+
+// Orders each row's hits by their hit coordinate (insertion sort; rows are short).
+__global__ void k_sort_rows(int64_t nrows, const int32_t* __restrict__ row_off, const int32_t* __restrict__ row_cnt,
+                            RowHit* hits) {
+  for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < nrows; row += (int64_t)gridDim.x * blockDim.x) {
+    RowHit* h = hits + row_off[row];
+    const int n = row_cnt[row];
+    for (int a = 1; a < n; ++a) {
+      const RowHit v = h[a];
+      int b = a - 1;
+      while (b >= 0 && h[b].key > v.key) { h[b + 1] = h[b]; --b; }
+      h[b + 1] = v;
+    }
+  }
+}
+
+// Number of distinct hits (gaps > eps) among sorted t values passing the direction's t > eps.
+__device__ __forceinline__ int clusters_pos(const double* ts, int n) {
+  int c = 0;
+  double prev = 0.0;
+  for (int a = 0; a < n; ++a) {
+    if (!(ts[a] > kEps)) continue;
+    if (c == 0 || fabs(ds(ts[a], prev)) > kEps) ++c;
+    prev = ts[a];
+  }
+  return c;
+}
+__device__ __forceinline__ int clusters_neg(const double* ts, int n) {
+  // the -axis ray sees t' = -t; ascending t' is descending t
+  int c = 0;
+  double prev = 0.0;
+  for (int a = n - 1; a >= 0; --a) {
+    const double tn = -ts[a];
+    if (!(tn > kEps)) continue;
+    if (c == 0 || fabs(ds(tn, prev)) > kEps) ++c;
+    prev = tn;
+  }
+  return c;
+}
+
+// Parities of the +AX / -AX rays of every node.  Thread order runs along the AX rows.
+// par bit0: +AX inside, bit1: -AX inside, bit7: row overflow (node takes the generic path).
+template <int AX>
+__global__ void __launch_bounds__(256) k_axis_parity(GridP g, int64_t row_base, const int32_t* __restrict__ row_off,
+                                                     const int32_t* __restrict__ row_cnt,
+                                                     const RowHit* __restrict__ hits, uint8_t* __restrict__ par) {
+  const int b = AX == 0 ? 1 : 0, c = AX == 2 ? 1 : 2;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < g.ngp; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t ia = t % g.n[AX];
+    const int64_t rest = t / g.n[AX];
+    const int64_t jb = rest % g.n[b], jc = rest / g.n[b];
+    int64_t idx[3];
+    idx[AX] = ia; idx[b] = jb; idx[c] = jc;
+    const int64_t lin = idx[0] + g.n[0] * (idx[1] + g.n[1] * idx[2]);
+    const int64_t row = row_base + jc * g.n[b] + jb;
+    const int32_t off = row_off[row], n = row_cnt[row];
+    if (n > kRowCap) { par[lin] = 0x80; continue; }
+    const double xa = da(g.o[AX], dm(g.h, (double)ia));
+    double ts[kRowCap];
+    for (int q = 0; q < n; ++q) {
+      const double tv = row_t<AX>(hits[off + q], xa);
+      int p = q - 1;
+      while (p >= 0 && ts[p] > tv) { ts[p + 1] = ts[p]; --p; }
+      ts[p + 1] = tv;
+    }
+    const int cp = clusters_pos(ts, n), cn = clusters_neg(ts, n);
+    par[lin] = (uint8_t)((cp & 1) | ((cn & 1) << 1));
+  }
+}
+
+// adaptive_point_in_mesh_raycast (:234-288).  cast(i) returns the parity of ray i (1-based) or
+// -1 when that ray is not available to the caller.
+template <class Cast>
+__device__ __forceinline__ int vote_logic(int min_rays, int max_rays, Cast cast, double& sign, double& conf,
+                                          int& total_out) {
+  int inside = 0, total = 0;
+  for (int i = 1; i <= min_rays; ++i) {
+    const int r = cast(i);
+    if (r < 0) return 1;
+    inside += r;
+    ++total;
+  }
+  double ratio = dd((double)inside, (double)total);
+  double cf = fmax(ratio, ds(1.0, ratio));
+  int used = min_rays;
+  while (cf < 0.85 && used < max_rays) {
+    const int batch = min(4, max_rays - used);
+    for (int i = used + 1; i <= used + batch; ++i) {
+      if (i <= 36) {
+        const int r = cast(i);
+        if (r < 0) return 1;
+        inside += r;
+        ++total;
+      }
+    }
+    used += batch;
+    ratio = dd((double)inside, (double)total);
+    cf = fmax(ratio, ds(1.0, ratio));
+    if (cf > 0.95) break;
+  }
+  sign = ratio > 0.5 ? 1.0 : -1.0;
+  conf = cf;
+  total_out = total;
+  return 0;
+}
+
+__device__ __forceinline__ int axis_bit(uint8_t px, uint8_t py, uint8_t pz, int i) {
+  // rays 1..6: +X +Y +Z -X -Y -Z
+  switch (i) {
+    case 1: return px & 1;
+    case 2: return py & 1;
+    case 3: return pz & 1;
+    case 4: return (px >> 1) & 1;
+    case 5: return (py >> 1) & 1;
+    default: return (pz >> 1) & 1;
+  }
+}
+
+struct VoteArgs {
+  GridP g;
+  const uint8_t* par[3];
+  int min_rays, max_rays;
+  double conf_thresh;
+  int use_winding;
+  double* sign;
+  double* conf;
+  int32_t* und_list;
+  int32_t* wind_list;
+  int64_t* counters;
+};
+
+__global__ void k_vote(VoteArgs A) {
+  const GridP& g = A.g;
+  for (int64_t lin = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; lin < g.ngp; lin += (int64_t)gridDim.x * blockDim.x) {
+    const uint8_t px = A.par[0][lin], py = A.par[1][lin], pz = A.par[2][lin];
+    const bool ovf = ((px | py | pz) & 0x80) != 0;
+    double s, cf;
+    int total;
+    const int rc = vote_logic(A.min_rays, A.max_rays,
+                              [&](int i) { return (i <= 6 && !ovf) ? axis_bit(px, py, pz, i) : -1; }, s, cf, total);
+    if (rc) {
+      const int64_t slot = atomicAdd((unsigned long long*)&A.counters[C_LIST_UNDECIDED], 1ULL);
+      A.und_list[slot] = (int32_t)lin;
+      continue;
+    }
+    if (A.use_winding && cf < A.conf_thresh) {
+      const int64_t slot = atomicAdd((unsigned long long*)&A.counters[C_LIST_WINDING], 1ULL);
+      A.wind_list[slot] = (int32_t)lin;
+      cf = 0.8;
+    }
+    A.sign[lin] = s;
+    if (A.conf) A.conf[lin] = cf;
+  }
+}
+
+struct RayArgs {
+  GridP g;
+  const BNode* nodes;
+  const int32_t* leaf_prim;
+  const TriRec64* rec;
+  float pad;
+  int64_t max_visits;
+  const uint8_t* par[3];
+  const int32_t* list;
+  int min_rays, max_rays;
+  double conf_thresh;
+  int use_winding;
+  double* sign;
+  double* conf;
+  int32_t* wind_list;
+  int64_t* counters;
+};
+
+__device__ __forceinline__ void child_box2(const BNode& nd, int side, float3& lo, float3& hi) {
+  if (side == 0) {
+    lo = make_float3(nd.a.x, nd.a.y, nd.a.z);
+    hi = make_float3(nd.a.w, nd.b.x, nd.b.y);
+  } else {
+    lo = make_float3(nd.b.z, nd.b.w, nd.c.x);
+    hi = make_float3(nd.c.y, nd.c.z, nd.c.w);
+  }
+}
+
+// check_ray_inside_bvh (:114-154) on the LBVH.  Returns parity, or -1 on buffer/stack overflow.
+__device__ int ray_parity(const RayArgs& A, const d3& p, const float3& p32, int dir) {
+  const d3 d = {c_dirs[3 * dir], c_dirs[3 * dir + 1], c_dirs[3 * dir + 2]};
+  const float3 d32 = make_float3((float)d.x, (float)d.y, (float)d.z);
+  const float3 inv = make_float3(1.0f / d32.x, 1.0f / d32.y, 1.0f / d32.z);
+  double ts[kRayCap];
+  int n = 0;
+  int stack[kStack];
+  int sp = 0;
+  stack[sp++] = 0;
+  int64_t visits = 0;
+  while (sp > 0) {
+    if (++visits > A.max_visits) return -1;
+    const BNode nd = A.nodes[stack[--sp]];
+    const int ch[2] = {nd.d.x, nd.d.y};
+    for (int side = 0; side < 2; ++side) {
+      float3 lo, hi;
+      child_box2(nd, side, lo, hi);
+      if (lo.x > hi.x) continue;
+      if (!ray_box(p32, d32, inv, lo, hi, A.pad, A.pad)) continue;
+      if (ch[side] & kLeafBit) {
+        const TriRec64& r = A.rec[A.leaf_prim[ch[side] & 0x7fffffff]];
+        double t;
+        if (mt64(p, d, rec_v(r, 0), rec_v(r, 1), rec_v(r, 2), kEps, t)) {
+          if (n >= kRayCap) return -1;
+          int q = n - 1;
+          while (q >= 0 && ts[q] > t) { ts[q + 1] = ts[q]; --q; }
+          ts[q + 1] = t;
+          ++n;
+        }
+      } else {
+        if (sp >= kStack) return -1;
+        stack[sp++] = ch[side];
+      }
+    }
+  }
+  if (n == 0) return 0;
+  int unique = 1;
+  for (int a = 1; a < n; ++a)
+    if (fabs(ds(ts[a], ts[a - 1])) > kEps) ++unique;
+  return unique & 1;
+}
+
+__global__ void __launch_bounds__(128) k_adaptive(RayArgs A) {
+  const GridP& g = A.g;
+  const int64_t count = A.counters[C_LIST_UNDECIDED];
+  int64_t rays = 0;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < count; q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t lin = A.list[q];
+    const int64_t i = lin % g.n[0], j = (lin / g.n[0]) % g.n[1], k = lin / (g.n[0] * g.n[1]);
+    const d3 p = node_coord(g.o, g.h, i, j, k);
+    const float3 p32 = make_float3((float)(p.x - g.center[0]), (float)(p.y - g.center[1]), (float)(p.z - g.center[2]));
+    const uint8_t px = A.par[0][lin], py = A.par[1][lin], pz = A.par[2][lin];
+    const bool ovf = ((px | py | pz) & 0x80) != 0;
+    bool bad = false;
+    double s, cf;
+    int total;
+    vote_logic(A.min_rays, A.max_rays,
+               [&](int r) {
+                 if (r <= 6 && !ovf) return axis_bit(px, py, pz, r);
+                 ++rays;
+                 const int v = ray_parity(A, p, p32, r - 1);
+                 if (v < 0) { bad = true; return 0; }
+                 return v;
+               },
+               s, cf, total);
+    if (bad) count_add(A.counters, C_ERR_CAPACITY, 1);
+    if (A.use_winding && cf < A.conf_thresh) {
+      const int64_t slot = atomicAdd((unsigned long long*)&A.counters[C_LIST_WINDING], 1ULL);
+      A.wind_list[slot] = (int32_t)lin;
+      cf = 0.8;
+    }
+    A.sign[lin] = s;
+    if (A.conf) A.conf[lin] = cf;
+  }
+  for (int off = 16; off > 0; off >>= 1) rays += __shfl_down_sync(0xffffffffu, rays, off);
+  if ((threadIdx.x & 31) == 0 && rays) count_add(A.counters, C_EXTRA_RAYS, rays);
+}
+
+// generalized_winding_number (:295-328): one CTA per node, fixed-order block reduction.
+__global__ void __launch_bounds__(256) k_winding(GridP g, const TriRec64* __restrict__ rec, int64_t nel,
+                                                 const int32_t* __restrict__ list, double* sign, int64_t* counters) {
+  __shared__ double red[256];
+  const int64_t count = counters[C_LIST_WINDING];
+  for (int64_t q = blockIdx.x; q < count; q += gridDim.x) {
+    const int64_t lin = list[q];
+    const int64_t i = lin % g.n[0], j = (lin / g.n[0]) % g.n[1], k = lin / (g.n[0] * g.n[1]);
+    const d3 p = node_coord(g.o, g.h, i, j, k);
+    double w = 0.0;
+    for (int64_t el = threadIdx.x; el < nel; el += blockDim.x) {
+      const TriRec64& r = rec[el];
+      const d3 a = v_normalize(v_sub(rec_v(r, 0), p));
+      const d3 b = v_normalize(v_sub(rec_v(r, 1), p));
+      const d3 c = v_normalize(v_sub(rec_v(r, 2), p));
+      const double num = v_dot(a, v_cross(b, c));
+      const double den = da(da(da(1.0, v_dot(a, b)), v_dot(b, c)), v_dot(c, a));
+      if (fabs(den) > 1e-10) {
+        double sa = dm(2.0, atan2(fabs(num), den));
+        if (num < 0) sa = -sa;
+        w = da(w, sa);
+      }
+    }
+    red[threadIdx.x] = w;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if ((int)threadIdx.x < s) red[threadIdx.x] = da(red[threadIdx.x], red[threadIdx.x + s]);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      const double wn = dd(red[0], 12.566370614359172);  // 4π
+      sign[lin] = fabs(wn) > 0.5 ? 1.0 : -1.0;
+      count_add(counters, C_WINDING, 1);
+      if (fabs(fabs(wn) - 0.5) < 1e-9) count_add(counters, C_WIND_AMBIG, 1);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_combine(int64_t n, const double* __restrict__ dist, const double* __restrict__ sign,
+                          double* __restrict__ sdf) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    sdf[q] = dm(dist[q], sign[q]);
+}
+
+}  // namespace
+
+int upload_directions(sdfgpu_ctx* ctx, const double* dirs) {
+  SDF_CUDA(ctx, cudaMemcpyToSymbolAsync(c_dirs, dirs, sizeof(double) * 108, 0, cudaMemcpyHostToDevice, ctx->stream));
+  return 0;
+}
+
+int run_signs(sdfgpu_ctx* ctx, const GridP& g, int min_rays, int max_rays, double conf_thresh, int use_winding,
+              const double* d_dist, double* d_sign, double* d_conf, double* d_sdf) {
+  cudaStream_t st = ctx->stream;
+  const MeshDev& M = ctx->mesh;
+  const int64_t nel = M.nel;
+  const TriRec64* rec = buf<TriRec64>(ctx, "rec");
+  const int64_t Rx = g.n[1] * g.n[2], Ry = g.n[0] * g.n[2], Rz = g.n[0] * g.n[1];
+  const int64_t nrows = Rx + Ry + Rz;
+  if (nrows >= 0x7fffffffLL) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "grid has too many rows");
+  int32_t *row_cnt, *row_off, *row_cur;
+  SDF_TRY(scratch_t(ctx, "row_cnt", (size_t)nrows + 1, &row_cnt));
+  SDF_TRY(scratch_t(ctx, "row_off", (size_t)nrows + 1, &row_off));
+  SDF_TRY(scratch_t(ctx, "row_cur", (size_t)nrows + 1, &row_cur));
+  SDF_CUDA(ctx, cudaMemsetAsync(row_cnt, 0, sizeof(int32_t) * (nrows + 1), st));
+  SDF_CUDA(ctx, cudaMemsetAsync(row_cur, 0, sizeof(int32_t) * (nrows + 1), st));
+  k_rows<<<grid_for(nel, 128), 128, 0, st>>>(rec, nel, g, Rx, Rx + Ry, false, row_cnt, nullptr, nullptr, nullptr,
+                                             ctx->d_counters);
+  SDF_CUDA(ctx, cudaGetLastError());
+  SDF_TRY(cub_scan_i32(ctx, row_cnt, row_off, nrows + 1));
+  int32_t total = 0;
+  SDF_CUDA(ctx, cudaMemcpyAsync(&total, row_off + nrows, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  SDF_CUDA(ctx, cudaStreamSynchronize(st));
+  if (total < 0) return fail(ctx, SDFGPU_ERR_CAPACITY, "more than 2^31 row hits");
+  RowHit* hits;
+  SDF_TRY(scratch_t(ctx, "row_hits", (size_t)std::max(total, 1), &hits));
+  if (total > 0) {
+    k_rows<<<grid_for(nel, 128), 128, 0, st>>>(rec, nel, g, Rx, Rx + Ry, true, nullptr, row_off, row_cur, hits,
+                                               ctx->d_counters);
+    SDF_CUDA(ctx, cudaGetLastError());
+    k_sort_rows<<<grid_for(nrows, 128), 128, 0, st>>>(nrows, row_off, row_cnt, hits);
+    SDF_CUDA(ctx, cudaGetLastError());
+  }
+  uint8_t *px, *py, *pz;
+  SDF_TRY(scratch_t(ctx, "par_x", (size_t)g.ngp, &px));
+  SDF_TRY(scratch_t(ctx, "par_y", (size_t)g.ngp, &py));
+  SDF_TRY(scratch_t(ctx, "par_z", (size_t)g.ngp, &pz));
+  const unsigned gp = grid_for(g.ngp, 256, 148 * 16);
+  k_axis_parity<0><<<gp, 256, 0, st>>>(g, 0, row_off, row_cnt, hits, px);
+  k_axis_parity<1><<<gp, 256, 0, st>>>(g, Rx, row_off, row_cnt, hits, py);
+  k_axis_parity<2><<<gp, 256, 0, st>>>(g, Rx + Ry, row_off, row_cnt, hits, pz);
+  SDF_CUDA(ctx, cudaGetLastError());
+
+  int32_t *und, *wind;
+  SDF_TRY(scratch_t(ctx, "und_list", (size_t)g.ngp, &und));
+  SDF_TRY(scratch_t(ctx, "wind_list", (size_t)g.ngp, &wind));
+  VoteArgs V;
+  V.g = g;
+  V.par[0] = px; V.par[1] = py; V.par[2] = pz;
+  V.min_rays = min_rays;
+  V.max_rays = max_rays;
+  V.conf_thresh = conf_thresh;
+  V.use_winding = use_winding;
+  V.sign = d_sign;
+  V.conf = d_conf;
+  V.und_list = und;
+  V.wind_list = wind;
+  V.counters = ctx->d_counters;
+  k_vote<<<grid_for(g.ngp, 256, 148 * 16), 256, 0, st>>>(V);
+  SDF_CUDA(ctx, cudaGetLastError());
+
+  RayArgs R;
+  R.g = g;
+  R.nodes = buf<BNode>(ctx, "nodes");
+  R.leaf_prim = buf<int32_t>(ctx, "leaf_prim");
+  R.rec = rec;
+  R.pad = (float)(2e-6 * g.E);
+  R.max_visits = 2 * nel + 64;
+  R.par[0] = px; R.par[1] = py; R.par[2] = pz;
+  R.list = und;
+  R.min_rays = min_rays;
+  R.max_rays = max_rays;
+  R.conf_thresh = conf_thresh;
+  R.use_winding = use_winding;
+  R.sign = d_sign;
+  R.conf = d_conf;
+  R.wind_list = wind;
+  R.counters = ctx->d_counters;
+  k_adaptive<<<148 * 8, 128, 0, st>>>(R);
+  SDF_CUDA(ctx, cudaGetLastError());
+  if (use_winding) {
+    k_winding<<<148 * 4, 256, 0, st>>>(g, rec, nel, wind, d_sign, ctx->d_counters);
+    SDF_CUDA(ctx, cudaGetLastError());
+  }
+  if (d_sdf && d_dist) {
+    k_combine<<<grid_for(g.ngp, 256, 148 * 16), 256, 0, st>>>(g.ngp, d_dist, d_sign, d_sdf);
+    SDF_CUDA(ctx, cudaGetLastError());
+  }
+  return 0;
+}
+
+}  // namespace sdfgpu

@@ -1,0 +1,231 @@
+"""ctypes binding of libsdfgpu.so (the C ABI declared in include/sdfgpu.h).
+
+The library is built in-tree into ``stl2sdf.jl_b200/lib/libsdfgpu.so`` (``make -C
+stl2sdf.jl_b200/csrc``).  There is no CPU fallback: if the library is missing or no sm_100
+device is present, every compute call raises :class:`SdfGpuError`.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.abspath(os.path.join(_PKG, "..", "lib", "libsdfgpu.so"))
+
+SDFGPU_OK = 0
+STATUS_NAMES = {
+    0: "OK", 1: "INVALID_ARGUMENT", 2: "NO_DEVICE", 3: "CUDA", 4: "OUT_OF_MEMORY", 5: "NO_MESH", 6: "CAPACITY", 7: "IO",
+}
+MODE_REF_RULE = 0
+MODE_EXACT = 1
+MODE_UNBOUNDED = 2
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+
+
+class SdfGpuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"sdfgpu error {code} ({STATUS_NAMES.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("tile", ctypes.c_int32 * 3)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("ngp", ctypes.c_int64), ("nel", ctypes.c_int64), ("tile_pairs", ctypes.c_int64),
+        ("active_tiles", ctypes.c_int64), ("candidate_nodes", ctypes.c_int64), ("fp64_evals", ctypes.c_int64),
+        ("knn_fallback_nodes", ctypes.c_int64), ("band_nodes", ctypes.c_int64), ("row_hits", ctypes.c_int64),
+        ("undecided_nodes", ctypes.c_int64), ("extra_rays", ctypes.c_int64), ("winding_nodes", ctypes.c_int64),
+        ("winding_ambiguous", ctypes.c_int64), ("unbounded_fallbacks", ctypes.c_int64), ("rho_max", ctypes.c_double),
+        ("ms_distance", ctypes.c_double), ("ms_sign", ctypes.c_double), ("ms_mesh", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# Every symbol include/sdfgpu.h declares, with its ctypes signature.
+SIGNATURES = {
+    "sdfgpu_abi_version": ([], ctypes.c_int),
+    "sdfgpu_create": ([ctypes.POINTER(Opts), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "sdfgpu_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "sdfgpu_last_error": ([ctypes.c_void_p], ctypes.c_char_p),
+    "sdfgpu_grid_setup": ([_dp, _dp, ctypes.c_int64, ctypes.c_int64, _dp, _dp, _i64p, _dp, _i64p], ctypes.c_int),
+    "sdfgpu_grid_from_cell_size": ([_dp, ctypes.c_int64, ctypes.c_double, _dp, _dp, _i64p, _dp, _i64p], ctypes.c_int),
+    "sdfgpu_set_mesh": ([ctypes.c_void_p, _dp, ctypes.c_int64, _i64p, ctypes.c_int64], ctypes.c_int),
+    "sdfgpu_set_mesh_device": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64],
+                               ctypes.c_int),
+    "sdfgpu_distances": ([ctypes.c_void_p, _dp, ctypes.c_double, _i64p, _dp, _dp, ctypes.c_int32, ctypes.c_int32],
+                         ctypes.c_int),
+    "sdfgpu_signs": ([ctypes.c_void_p, _dp, ctypes.c_double, _i64p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                      ctypes.c_int32, _dp, _dp], ctypes.c_int),
+    "sdfgpu_sdf": ([ctypes.c_void_p, _dp, ctypes.c_double, _i64p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                    ctypes.c_double, ctypes.c_int32, _dp, _dp, _dp, _dp], ctypes.c_int),
+    "sdfgpu_sdf_device": ([ctypes.c_void_p, _dp, ctypes.c_double, _i64p, ctypes.c_int32, ctypes.c_int32,
+                           ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                           ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "sdfgpu_get_stream": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "sdfgpu_get_stats": ([ctypes.c_void_p, ctypes.POINTER(Stats)], ctypes.c_int),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib():
+    """Load libsdfgpu.so (raises if it has not been built)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise SdfGpuError(7, f"{LIB_PATH} is missing; build it with `make -C stl2sdf.jl_b200/csrc`")
+            L = ctypes.CDLL(LIB_PATH)
+            for name, (args, res) in SIGNATURES.items():
+                fn = getattr(L, name)
+                fn.argtypes = args
+                fn.restype = res
+            _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    return a.ctypes.data_as(_i64p)
+
+
+def grid_setup(xmin, xmax, n_max, margin=3):
+    o = np.zeros(3); amax = np.zeros(3); N = np.zeros(3, np.int64); h = ctypes.c_double(); ngp = ctypes.c_int64()
+    rc = lib().sdfgpu_grid_setup(_d(np.ascontiguousarray(xmin, np.float64)), _d(np.ascontiguousarray(xmax, np.float64)),
+                                 int(n_max), int(margin), _d(o), _d(amax), _i(N), ctypes.byref(h), ctypes.byref(ngp))
+    if rc:
+        raise SdfGpuError(rc, "grid setup rejected its arguments (need finite bounds, positive extent, N_max >= 1)")
+    return o, amax, N, h.value, ngp.value
+
+
+def grid_from_cell_size(X, B):
+    X = np.ascontiguousarray(X, np.float64).reshape(-1, 3)
+    o = np.zeros(3); amax = np.zeros(3); N = np.zeros(3, np.int64); h = ctypes.c_double(); ngp = ctypes.c_int64()
+    rc = lib().sdfgpu_grid_from_cell_size(_d(X), X.shape[0], float(B), _d(o), _d(amax), _i(N), ctypes.byref(h),
+                                          ctypes.byref(ngp))
+    if rc:
+        raise SdfGpuError(rc, "grid setup rejected its arguments (cell size must be > 0 and below the mesh extent)")
+    return o, amax, N, h.value, ngp.value
+
+
+class Context:
+    """One libsdfgpu context (one CUDA device, one stream, resident mesh)."""
+
+    def __init__(self, device: int = 0, tile=(0, 0, 0)):
+        L = lib()
+        opts = Opts(device, (ctypes.c_int32 * 3)(*tile))
+        p = ctypes.c_void_p()
+        rc = L.sdfgpu_create(ctypes.byref(opts), ctypes.byref(p))
+        if rc:
+            raise SdfGpuError(rc, L.sdfgpu_last_error(None).decode())
+        self._p = p
+        self._mesh_key = None
+
+    def _check(self, rc):
+        if rc:
+            raise SdfGpuError(rc, lib().sdfgpu_last_error(self._p).decode())
+
+    def close(self):
+        if self._p:
+            lib().sdfgpu_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._p
+
+    def stream_ptr(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(lib().sdfgpu_get_stream(self._p, ctypes.byref(s)))
+        return int(s.value or 0)
+
+    def set_mesh(self, X, IEN, key=None):
+        """X: (nnp, 3) float64; IEN: (nel, 3) int64 1-based (vertex-major = 3 x n column-major)."""
+        if key is not None and key == self._mesh_key:
+            return
+        X = np.ascontiguousarray(X, np.float64).reshape(-1, 3)
+        IEN = np.ascontiguousarray(IEN, np.int64).reshape(-1, 3)
+        self._check(lib().sdfgpu_set_mesh(self._p, _d(X), X.shape[0], _i(IEN), IEN.shape[0]))
+        self._mesh_key = key
+
+    def set_mesh_device(self, x_ptr: int, nnp: int, ien_ptr: int, nel: int):
+        self._check(lib().sdfgpu_set_mesh_device(self._p, ctypes.c_void_p(x_ptr), nnp, ctypes.c_void_p(ien_ptr), nel))
+        self._mesh_key = None
+
+    def distances(self, origin, h, N, mode=MODE_REF_RULE, want_xp=False, learned=False, out=None):
+        N = np.ascontiguousarray(N, np.int64)
+        origin = np.ascontiguousarray(origin, np.float64)
+        ngp = int(np.prod(N + 1))
+        dist = np.empty(ngp) if out is None else out
+        xp = np.empty((ngp, 3)) if want_xp else None
+        self._check(lib().sdfgpu_distances(self._p, _d(origin), float(h), _i(N), _d(dist),
+                                           _d(xp) if xp is not None else None, int(mode), int(bool(learned))))
+        return dist, xp
+
+    def signs(self, origin, h, N, min_rays=6, max_rays=30, confidence_threshold=0.6, use_winding_fallback=True):
+        N = np.ascontiguousarray(N, np.int64)
+        origin = np.ascontiguousarray(origin, np.float64)
+        ngp = int(np.prod(N + 1))
+        sign = np.empty(ngp); conf = np.empty(ngp)
+        self._check(lib().sdfgpu_signs(self._p, _d(origin), float(h), _i(N), int(min_rays), int(max_rays),
+                                       float(confidence_threshold), int(bool(use_winding_fallback)), _d(sign), _d(conf)))
+        return sign, conf
+
+    def sdf(self, origin, h, N, mode=MODE_REF_RULE, min_rays=6, max_rays=30, confidence_threshold=0.6,
+            use_winding_fallback=True, want_parts=False):
+        N = np.ascontiguousarray(N, np.int64)
+        origin = np.ascontiguousarray(origin, np.float64)
+        ngp = int(np.prod(N + 1))
+        sdf = np.empty(ngp)
+        parts = [np.empty(ngp) for _ in range(3)] if want_parts else [None, None, None]
+        self._check(lib().sdfgpu_sdf(self._p, _d(origin), float(h), _i(N), int(mode), int(min_rays), int(max_rays),
+                                     float(confidence_threshold), int(bool(use_winding_fallback)), _d(sdf),
+                                     *[(_d(p) if p is not None else None) for p in parts]))
+        return (sdf, *parts) if want_parts else sdf
+
+    def sdf_device(self, origin, h, N, sdf_ptr, mode=MODE_REF_RULE, min_rays=6, max_rays=30,
+                   confidence_threshold=0.6, use_winding_fallback=True, dist_ptr=0, sign_ptr=0, conf_ptr=0):
+        N = np.ascontiguousarray(N, np.int64)
+        origin = np.ascontiguousarray(origin, np.float64)
+        self._check(lib().sdfgpu_sdf_device(self._p, _d(origin), float(h), _i(N), int(mode), int(min_rays),
+                                            int(max_rays), float(confidence_threshold),
+                                            int(bool(use_winding_fallback)), ctypes.c_void_p(sdf_ptr),
+                                            ctypes.c_void_p(dist_ptr or None), ctypes.c_void_p(sign_ptr or None),
+                                            ctypes.c_void_p(conf_ptr or None)))
+
+    def stats(self) -> dict:
+        s = Stats()
+        self._check(lib().sdfgpu_get_stats(self._p, ctypes.byref(s)))
+        return s.as_dict()
+
+
+_default_ctx = {}
+
+
+def default_context(device: int = 0) -> Context:
+    ctx = _default_ctx.get(device)
+    if ctx is None:
+        ctx = Context(device)
+        _default_ctx[device] = ctx
+    return ctx
