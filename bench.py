@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Benchmark of the SignedDistances hot path on B200: SDF grid nodes/s.
+
+One step = one pass of the hot path over the workload: build the acceleration data from the
+device-resident mesh (sdfgpu_set_mesh_device: triangle records + LBVH) and compute distances,
+signs and sdf = dist .* sign for every grid node (sdfgpu_sdf_device).  The reference does the
+same work per call (KD-trees and BVH are built inside evalDistancesOnTriMesh and
+raycast_sign_detection).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload torus128|icosphere|...]
+    python bench.py --impl reference ...   # the reference algorithm on the host cores
+
+Multi-GPU (torchrun, one rank per GPU): every rank computes its own copy of the workload (weak
+scaling, no data-path collective); value = nodes of all ranks / max-over-ranks device time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "stl2sdf.jl_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "SDF grid nodes/s on 1 B200: learned-radius vs plain GPU vs CPU ref, sign exact"
+
+
+def make_workload(name: str):
+    """(X, IEN, grid dict, description) of a named workload, read back through float32 STL."""
+    import numpy as np
+
+    from stl2sdf import DataImport, _native, synthetic
+
+    if name == "icosphere":
+        V, F = synthetic.icosphere(4, jitter=0.01, seed=0)
+        X, IEN = DataImport.roundtrip_float32(V, F)
+        o, amax, N, h, ngp = _native.grid_from_cell_size(X, 0.05)
+        desc = "icosphere L4 (5120 tris) r=1 jitter N(0,0.01) seed 0, cell_size 0.05, pad 3"
+    elif name == "torus128":
+        V, F = synthetic.torus(1.0, 0.3, 512, 128, 0.02, seed=1)
+        X, IEN = DataImport.roundtrip_float32(V, F)
+        o, amax, N, h, ngp = _native.grid_setup(X.min(0), X.max(0), 128 - 7, 3)
+        desc = "torus R=1 r=0.3 512x128 quads (131072 tris) noise U(-2%,2%) seed 1, 128 nodes on the long axis"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    g = dict(origin=np.asarray(o), N=np.asarray(N), h=float(h), ngp=int(ngp))
+    return X, IEN, g, desc
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._proc = None
+
+    def __enter__(self):
+        q = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+            "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                           "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (OSError, FileNotFoundError):
+            self._proc = None
+        return self
+
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+
+    def summary(self):
+        import statistics
+
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def cpu_baseline(X, IEN, g, budget_s=12.0, seed=42):
+    """The oracle (C++ FP64 restatement of the reference, all host threads) on a seeded node
+    sample of the workload grid, doubled until it takes >= budget_s or covers the grid."""
+    import numpy as np
+
+    import oracle
+
+    nthreads = oracle.max_threads()
+    k = 1 << 14
+    rng = np.random.default_rng(seed)
+    while True:
+        nodes = np.sort(rng.choice(g["ngp"], size=min(k, g["ngp"]), replace=False)).astype(np.int64)
+        t0 = time.perf_counter()
+        oracle.distances(X, IEN, g["origin"], g["h"], g["N"], mode=0, nodes=nodes, nthreads=nthreads)
+        oracle.signs(X, IEN, g["origin"], g["h"], g["N"], nodes=nodes, nthreads=nthreads)
+        dt = time.perf_counter() - t0
+        if dt >= budget_s or nodes.shape[0] >= g["ngp"] or k >= (1 << 24):
+            break
+        k *= 2
+    return {"value": nodes.shape[0] / dt, "unit": "nodes/s", "cores": nthreads, "kind": "port",
+            "sample": f"{nodes.shape[0]} seeded (seed {seed}) uniform grid nodes of the workload, distance+sign, {dt:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference algorithm (the oracle restatement) on the host cores."""
+    if rank != 0:
+        return 0
+    import numpy as np
+
+    import oracle
+
+    X, IEN, g, desc = make_workload(args.workload)
+    nthreads = oracle.max_threads()
+    sample = min(g["ngp"], args.ref_sample)
+    rng = np.random.default_rng(7)
+    times = []
+    for step in range(args.warmup + args.steps):
+        nodes = np.sort(rng.choice(g["ngp"], size=sample, replace=False)).astype(np.int64)
+        t0 = time.perf_counter()
+        oracle.distances(X, IEN, g["origin"], g["h"], g["N"], mode=0, nodes=nodes, nthreads=nthreads)
+        oracle.signs(X, IEN, g["origin"], g["h"], g["N"], nodes=nodes, nthreads=nthreads)
+        if step >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = sample * len(times) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "nodes/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "description": desc, "ngp": g["ngp"], "nel": int(IEN.shape[0]),
+                   "step": f"distance+sign of {sample} seeded grid nodes"},
+        "cpu_baseline": {"value": value, "unit": "nodes/s", "cores": nthreads, "kind": "port",
+                         "sample": f"{sample} seeded grid nodes per step, distance+sign"},
+        "e2e": {"value": value, "unit": "nodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="sdfgpu", choices=["sdfgpu", "reference"])
+    ap.add_argument("--workload", default="torus128")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-sample", type=int, default=1 << 14)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+
+    from stl2sdf import _native
+
+    torch.cuda.set_device(local)
+    dist_on = world > 1
+    if dist_on:
+        import datetime
+
+        import torch.distributed as tdist
+
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    X, IEN, g, desc = make_workload(args.workload)
+    ngp = g["ngp"]
+    ctx = _native.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=f"cuda:{local}")
+    dev = torch.device(f"cuda:{local}")
+    dX = torch.from_numpy(np.ascontiguousarray(X)).to(dev)
+    dIEN = torch.from_numpy(np.ascontiguousarray(IEN)).to(dev)
+    out = torch.empty(ngp, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    torch.cuda.synchronize()
+
+    def step():
+        ctx.set_mesh_device(dX.data_ptr(), X.shape[0], dIEN.data_ptr(), IEN.shape[0])
+        ctx.sdf_device(g["origin"], g["h"], g["N"], out.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+    torch.cuda.synchronize()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    fold_ms, launches, mesh_launches = [], 0, 0
+    if dist_on:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter()
+    with ClockSampler(local) as clk:
+        for s in range(args.steps):
+            starts[s].record(stream)
+            step()
+            ends[s].record(stream)
+            st = ctx.stats()
+            fold_ms.append(st["ms_fold"])
+            launches += st["launches"]
+            mesh_launches += st["mesh_launches"]
+            with torch.cuda.stream(stream):
+                flush.fill_(s & 0xFF)
+        torch.cuda.synchronize()
+        if dist_on:
+            tdist.barrier()
+    wall = time.perf_counter() - t_wall
+    dev_ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
+    if dist_on:
+        tt = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
+        tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
+        dev_ms = float(tt.item())
+    value = ngp * args.steps * world / (dev_ms / 1e3)
+    stats = ctx.stats()
+
+    # End to end through the public C ABI with pinned host buffers: H2D of the mesh, all stages,
+    # D2H of the sdf, every step.
+    hX = torch.from_numpy(np.ascontiguousarray(X)).pin_memory()
+    hIEN = torch.from_numpy(np.ascontiguousarray(IEN)).pin_memory()
+    hout = torch.empty(ngp, dtype=torch.float64).pin_memory()
+    import ctypes
+
+    L = _native.lib()
+    o = np.ascontiguousarray(g["origin"], np.float64)
+    N = np.ascontiguousarray(g["N"], np.int64)
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int64)
+
+    def e2e_step():
+        rc = L.sdfgpu_set_mesh(ctx.handle, ctypes.cast(hX.data_ptr(), dp), X.shape[0], ctypes.cast(hIEN.data_ptr(), ip),
+                               IEN.shape[0])
+        rc = rc or L.sdfgpu_sdf(ctx.handle, o.ctypes.data_as(dp), g["h"], N.ctypes.data_as(ip), 0, 6, 30, 0.6, 1,
+                                ctypes.cast(hout.data_ptr(), dp), None, None, None)
+        if rc:
+            raise _native.SdfGpuError(rc, L.sdfgpu_last_error(ctx.handle).decode())
+
+    for _ in range(2):
+        e2e_step()
+    e2e_steps = max(3, min(args.steps, 20))
+    es, ee = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    es.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    ee.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = es.elapsed_time(ee)
+    if dist_on:
+        tt = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    e2e_value = ngp * e2e_steps * world / (e2e_ms / 1e3)
+    assert np.array_equal(hout.numpy(), out.cpu().numpy()), "e2e and device-resident results differ"
+
+    # Roofline of the dominant kernel (the tile fold): algorithmic bytes per launch = node outputs
+    # (dist 8 B + status 1 B per node) + the sorted (tile, triangle) list (4 B per pair) + the
+    # triangle data read once (FP64 record 352 B + FP32 vertices 48 B + centroids 48 B).
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peaks = json.load(open(peaks_path))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    fold_avg = sum(fold_ms) / len(fold_ms)
+    alg_bytes = 9 * ngp + 4 * stats["tile_pairs"] + 448 * IEN.shape[0]
+    achieved = alg_bytes / (fold_avg / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(args.workload, {}).get("k_tile_fold")
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "nodes/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "description": desc, "ngp": ngp, "nel": int(IEN.shape[0]),
+                   "N": [int(v) for v in g["N"]], "mode": "ref-rule", "l2": "flushed between steps (256 MB write)",
+                   "step": "set_mesh_device (triangle records + LBVH) + sdf_device (distance, sign, combine)"},
+        "e2e": {"value": e2e_value, "unit": "nodes/s", "h2d_bytes_per_step": int(X.nbytes + IEN.nbytes),
+                "d2h_bytes_per_step": int(ngp * 8)},
+        "gpu_launches": int(launches + mesh_launches),
+        "roofline": {"bound": "hbm", "kernel": "k_tile_fold", "achieved": achieved, "peak": peak,
+                     "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "alg_bytes_per_launch": int(alg_bytes), "ms_per_launch": fold_avg},
+        "stages_ms": {k: stats[k] for k in ("ms_mesh", "ms_tiles", "ms_fold", "ms_rows", "ms_parity", "ms_vote",
+                                             "ms_distance", "ms_sign")},
+        "counters": {k: stats[k] for k in ("tile_pairs", "fp64_evals", "candidate_nodes", "row_hits",
+                                            "undecided_nodes", "extra_rays", "winding_nodes", "knn_fallback_nodes")},
+        "clocks": clk.summary(),
+        "wall_s": wall,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(X, IEN, g)
+    if dist_on:
+        tdist.barrier()
+        tdist.destroy_process_group()
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -93,6 +93,13 @@ typedef struct sdfgpu_stats {
   double ms_distance;             /* device time of the distance stage (ms) */
   double ms_sign;                 /* device time of the sign stage (ms) */
   double ms_mesh;                 /* device time of the last set_mesh (ms) */
+  int64_t launches;               /* kernels of this library launched by the last call (CUB excluded) */
+  int64_t mesh_launches;          /* same, for the last set_mesh */
+  double ms_tiles;                /* (tile, triangle) pair build + sort */
+  double ms_fold;                 /* tile fold kernel (the distance hot loop) */
+  double ms_rows;                 /* axis-row hit lists (count, fill, sort) */
+  double ms_parity;               /* the three axis-parity kernels */
+  double ms_vote;                 /* vote + adaptive rays + winding */
 } sdfgpu_stats;
 
 /* Context lifetime.  opts may be NULL (device 0, default tiles). */

@@ -224,21 +224,34 @@ int check_mode(sdfgpu_ctx* ctx, int mode, int learned) {
 int run_all(sdfgpu_ctx* ctx, const GridP& g, bool want_dist, bool want_sign, int mode, int learned, int min_rays,
             int max_rays, double conf, int use_winding, double* d_dist, double* d_xp, double* d_sign, double* d_conf,
             double* d_sdf) {
-  cudaStream_t st = ctx->stream;
   SDF_TRY(reset_counters(ctx));
-  SDF_CUDA(ctx, cudaEventRecord(ctx->ev[0], st));
+  ctx->launches = 0;
+  for (int i = 0; i < T_NUM; ++i) SDF_MARK(ctx, i);
   if (want_dist) SDF_TRY(run_distances(ctx, g, mode, learned, d_dist, d_xp));
-  SDF_CUDA(ctx, cudaEventRecord(ctx->ev[1], st));
+  SDF_MARK(ctx, T_DIST1);
+  for (int i = T_ROWS; i < T_NUM; ++i) SDF_MARK(ctx, i);
   // Rays past the 36th are never cast, so every max_rays >= 44 gives the same votes as 44.
   const int max_eff = max_rays > 44 ? 44 : max_rays;
   if (want_sign) SDF_TRY(run_signs(ctx, g, min_rays, max_eff, conf, use_winding, d_dist, d_sign, d_conf, d_sdf));
-  SDF_CUDA(ctx, cudaEventRecord(ctx->ev[2], st));
+  SDF_MARK(ctx, T_SIGN1);
   SDF_TRY(finish_counters(ctx, g));
-  float a = 0.f, b = 0.f;
-  SDF_CUDA(ctx, cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]));
-  SDF_CUDA(ctx, cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]));
-  ctx->stats.ms_distance = want_dist ? a : 0.0;
-  ctx->stats.ms_sign = want_sign ? b : 0.0;
+  auto span = [&](int a, int b, double* out) -> int {
+    float ms = 0.f;
+    SDF_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->tev[a], ctx->tev[b]));
+    *out = ms > 0.f ? ms : 0.0;
+    return 0;
+  };
+  sdfgpu_stats& s = ctx->stats;
+  SDF_TRY(span(T_DIST0, T_DIST1, &s.ms_distance));
+  SDF_TRY(span(T_DIST1, T_SIGN1, &s.ms_sign));
+  SDF_TRY(span(T_DIST0, T_TILES, &s.ms_tiles));
+  SDF_TRY(span(T_TILES, T_FOLD, &s.ms_fold));
+  SDF_TRY(span(T_DIST1, T_ROWS, &s.ms_rows));
+  SDF_TRY(span(T_ROWS, T_PARITY, &s.ms_parity));
+  SDF_TRY(span(T_PARITY, T_SIGN1, &s.ms_vote));
+  if (!want_dist) s.ms_distance = s.ms_tiles = s.ms_fold = 0.0;
+  if (!want_sign) s.ms_sign = s.ms_rows = s.ms_parity = s.ms_vote = 0.0;
+  s.launches = ctx->launches;
   return 0;
 }
 
@@ -274,9 +287,10 @@ int sdfgpu_create(const sdfgpu_opts* opts, sdfgpu_ctx** out) {
   if (opts)
     for (int a = 0; a < 3; ++a)
       if (opts->tile[a] > 0) ctx->tile[a] = opts->tile[a];
-  if (ctx->tile[0] * ctx->tile[1] * ctx->tile[2] > 256 || ctx->tile[0] * ctx->tile[1] * ctx->tile[2] < 1) {
+  const int tn = ctx->tile[0] * ctx->tile[1] * ctx->tile[2];
+  if (tn > 256 || tn < 32 || tn % 32 != 0) {
     delete ctx;
-    return fail(nullptr, SDFGPU_ERR_INVALID_ARGUMENT, "tile must hold 1..256 nodes");
+    return fail(nullptr, SDFGPU_ERR_INVALID_ARGUMENT, "a tile must hold 32, 64, ..., 256 nodes");
   }
   auto bail = [&](const char* what, cudaError_t err) {
     std::string m = std::string(what) + ": " + cudaGetErrorString(err);
@@ -286,6 +300,8 @@ int sdfgpu_create(const sdfgpu_opts* opts, sdfgpu_ctx** out) {
   if ((e = cudaSetDevice(dev)) != cudaSuccess) return bail("cudaSetDevice", e);
   if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail("cudaStreamCreate", e);
   for (auto& ev : ctx->ev)
+    if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail("cudaEventCreate", e);
+  for (auto& ev : ctx->tev)
     if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail("cudaEventCreate", e);
   if ((e = cudaMalloc(&ctx->d_counters, sizeof(int64_t) * C_NUM)) != cudaSuccess) return bail("cudaMalloc", e);
   double D[36][3];
@@ -308,6 +324,8 @@ int sdfgpu_destroy(sdfgpu_ctx* ctx) {
     if (kv.second.p) cudaFree(kv.second.p);
   if (ctx->d_counters) cudaFree(ctx->d_counters);
   for (auto& ev : ctx->ev)
+    if (ev) cudaEventDestroy(ev);
+  for (auto& ev : ctx->tev)
     if (ev) cudaEventDestroy(ev);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;

@@ -87,6 +87,8 @@ struct sdfgpu_ctx {
   int64_t* d_counters = nullptr;
   int64_t h_counters[sdfgpu::C_NUM] = {};
   sdfgpu_stats stats = {};
+  int64_t launches = 0;  // kernels of this library launched since the last reset
+  cudaEvent_t tev[8] = {};  // stage timestamps, see sdfgpu::Stage
 };
 
 namespace sdfgpu {
@@ -102,6 +104,17 @@ int fail(sdfgpu_ctx* ctx, int code, const std::string& msg);
                             std::string(#call) + ": " + cudaGetErrorString(e__));                 \
     }                                                                                             \
   } while (0)
+
+// Checks a kernel launch and counts it.
+#define SDF_KERNEL(ctx)                         \
+  do {                                          \
+    SDF_CUDA((ctx), cudaGetLastError());        \
+    ++(ctx)->launches;                          \
+  } while (0)
+
+// Stage timestamps recorded on the context stream.
+enum Stage : int { T_DIST0 = 0, T_TILES, T_FOLD, T_DIST1, T_ROWS, T_PARITY, T_SIGN1, T_NUM };
+#define SDF_MARK(ctx, i) SDF_CUDA((ctx), cudaEventRecord((ctx)->tev[(i)], (ctx)->stream))
 
 #define SDF_TRY(expr)          \
   do {                         \

@@ -140,50 +140,92 @@ struct FoldArgs {
   int64_t* counters;
 };
 
+// Per-warp shared staging of 32 list entries: FP32 vertices and centroid (64 B each) and, per
+// (entry, lane), the FP32 distance that passed the filter.
+struct __align__(16) WarpStage {
+  float4 v[32][3];
+  float4 c[32];
+  int32_t id[32];
+  float D[32][32];  // [entry][lane]
+};
+
+// One CTA per tile, one lane per node.  The tile's ascending triangle list is consumed 32 entries
+// at a time.  Phase A (convergent FP32): every lane tests each staged entry against its own node
+// (centroid ball, then point-triangle distance D against the running minimum m) and sets a bit
+// per surviving entry.  Phase B: lanes drain their bits lowest-first, i.e. in ascending triangle
+// index, so all lanes execute the FP64 reference step together on different triangles instead of
+// one lane at a time; an entry whose D now exceeds the (smaller) running minimum is dropped.
 __global__ void __launch_bounds__(256) k_tile_fold(FoldArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpStage& S = reinterpret_cast<WarpStage*>(smem_raw)[threadIdx.x >> 5];
+  const unsigned lane = threadIdx.x & 31;
   const GridP& g = A.g;
   const int64_t tile = blockIdx.x;
   const int64_t tx = tile % g.nt[0], ty = (tile / g.nt[0]) % g.nt[1], tz = tile / (g.nt[0] * g.nt[1]);
   const int lx = threadIdx.x % g.t[0], ly = (threadIdx.x / g.t[0]) % g.t[1], lz = threadIdx.x / (g.t[0] * g.t[1]);
   const int64_t i = tx * g.t[0] + lx, j = ty * g.t[1] + ly, k = tz * g.t[2] + lz;
   const bool valid = i <= g.N[0] && j <= g.N[1] && k <= g.N[2];
+  const int64_t lin = i + g.n[0] * (j + g.n[1] * k);
+  const d3 p = node_coord(g.o, g.h, i, j, k);
+  const float3 p32 = local32(g, p);
+  const int32_t start = A.tile_off[tile], end = start + A.tile_cnt[tile];
+  const bool ref = A.mode == SDFGPU_MODE_REF_RULE;
+  double m = kBig;
+  d3 proj = {0.0, 0.0, 0.0};
+  bool have = false, any = false;
   int64_t fp64 = 0;
-  int cand = 0;
-  if (valid) {
-    const int64_t lin = i + g.n[0] * (j + g.n[1] * k);
-    const d3 p = node_coord(g.o, g.h, i, j, k);
-    const float3 p32 = local32(g, p);
-    const int32_t start = A.tile_off[tile], cnt = A.tile_cnt[tile];
-    double m = kBig;
-    d3 proj = {0.0, 0.0, 0.0};
-    bool have = false, any = false;
-    const bool ref = A.mode == SDFGPU_MODE_REF_RULE;
-    for (int32_t e = start; e < start + cnt; ++e) {
-      const int32_t tri = __ldg(&A.vals[e]);
-      if (ref) {
-        const float4 c = __ldg(&A.c32[tri]);
-        const float dx = c.x - p32.x, dy = c.y - p32.y, dz = c.z - p32.z;
-        const float s32 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        if (s32 > A.r2_out) continue;
-        if (s32 >= A.r2_in) {  // inside the FP32 error band: the reference's FP64 test decides
-          const double4 cc = A.cent[tri];
-          const double ex = ds(cc.x, p.x), ey = ds(cc.y, p.y), ez = ds(cc.z, p.z);
-          double s = dm(ex, ex);
-          s = da(s, dm(ey, ey));
-          s = da(s, dm(ez, ez));
-          if (!(s <= A.r2)) continue;
+  for (int32_t base = start; base < end; base += 32) {
+    const int nE = min(32, end - base);
+    if ((int)lane < nE) {
+      const int32_t tri = __ldg(&A.vals[base + lane]);
+      S.id[lane] = tri;
+      S.v[lane][0] = __ldg(&A.v32[3 * tri]);
+      S.v[lane][1] = __ldg(&A.v32[3 * tri + 1]);
+      S.v[lane][2] = __ldg(&A.v32[3 * tri + 2]);
+      S.c[lane] = __ldg(&A.c32[tri]);
+    }
+    __syncwarp();
+    uint32_t bits = 0;
+    if (valid) {
+      const float lim = have ? (float)m + A.eD_abs + A.eD_rel * (float)m : 3.0e38f;
+      for (int q = 0; q < nE; ++q) {
+        if (ref) {
+          const float4 c = S.c[q];
+          const float dx = c.x - p32.x, dy = c.y - p32.y, dz = c.z - p32.z;
+          const float s32 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+          if (s32 > A.r2_out) continue;
+          if (s32 >= A.r2_in) {  // inside the FP32 error band: the reference's FP64 test decides
+            const double4 cc = A.cent[S.id[q]];
+            const double ex = ds(cc.x, p.x), ey = ds(cc.y, p.y), ez = ds(cc.z, p.z);
+            double s = dm(ex, ex);
+            s = da(s, dm(ey, ey));
+            s = da(s, dm(ez, ez));
+            if (!(s <= A.r2)) continue;
+          }
+        }
+        any = true;
+        const float D = sqrtf(pt_tri_d2(p32, f3(S.v[q][0]), f3(S.v[q][1]), f3(S.v[q][2])));
+        if (D <= lim) {
+          bits |= 1u << q;
+          S.D[q][lane] = D;
         }
       }
-      any = true;
-      if (have) {
-        const float D = sqrtf(pt_tri_d2(p32, f3(__ldg(&A.v32[3 * tri])), f3(__ldg(&A.v32[3 * tri + 1])),
-                                        f3(__ldg(&A.v32[3 * tri + 2]))));
-        if ((double)D > m + (double)(A.eD_abs + A.eD_rel * (float)m)) continue;
-      }
-      tri_step64(A.rec[tri], p, m, proj, ref);
-      have = true;
-      ++fp64;
     }
+    while (__any_sync(0xffffffffu, bits != 0)) {
+      if (bits) {
+        const int q = __ffs(bits) - 1;
+        bits &= bits - 1;
+        if (!have || (double)S.D[q][lane] <= m + (double)(A.eD_abs + A.eD_rel * (float)m)) {
+          tri_step64(A.rec[S.id[q]], p, m, proj, ref);
+          have = true;
+          ++fp64;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  int cand = 0;
+  if (valid) {
     double d = m;
     if (fabs(d) > fabs(g.h)) d = g.h;  // clamp (dfOnTriangularMesh.jl:202-206)
     A.dist[lin] = d;
@@ -200,7 +242,7 @@ __global__ void __launch_bounds__(256) k_tile_fold(FoldArgs A) {
     fp64 += __shfl_down_sync(0xffffffffu, fp64, off);
     cand += __shfl_down_sync(0xffffffffu, cand, off);
   }
-  if ((threadIdx.x & 31) == 0) {
+  if (lane == 0) {
     if (fp64) count_add(A.counters, C_FP64, fp64);
     if (cand) count_add(A.counters, C_CAND_NODES, cand);
   }
@@ -454,8 +496,10 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
   if (mode == SDFGPU_MODE_UNBOUNDED) {
     (void)use_learned;
     UnbArgs A{g, nodes, leaf_prim, v32, rec, pad, eD_abs, eD_rel, 2 * nel + 64, d_dist, d_xp, ctx->d_counters};
+    SDF_MARK(ctx, T_TILES);
     k_unbounded<<<grid_for(g.ngp, 128, 148 * 32), 128, 0, st>>>(A);
-    SDF_CUDA(ctx, cudaGetLastError());
+    SDF_KERNEL(ctx);
+    SDF_MARK(ctx, T_FOLD);
     return 0;
   }
 
@@ -473,7 +517,7 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
   SDF_CUDA(ctx, cudaMemsetAsync(tri_cnt + nel, 0, sizeof(int32_t), st));
   k_tile_pairs<false><<<grid_for(nel, 128), 128, 0, st>>>(cent, rec, nel, g, mode, R, tri_cnt, nullptr, tile_cnt,
                                                           nullptr, nullptr);
-  SDF_CUDA(ctx, cudaGetLastError());
+  SDF_KERNEL(ctx);
   SDF_TRY(cub_scan_i32(ctx, tri_cnt, tri_off, nel + 1));
   int32_t total = 0;
   SDF_CUDA(ctx, cudaMemcpyAsync(&total, tri_off + nel, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
@@ -488,7 +532,7 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
   if (total > 0) {
     k_tile_pairs<true><<<grid_for(nel, 128), 128, 0, st>>>(cent, rec, nel, g, mode, R, nullptr, tri_off, nullptr,
                                                            keys, vals);
-    SDF_CUDA(ctx, cudaGetLastError());
+    SDF_KERNEL(ctx);
     const int bits = ceil_log2((uint64_t)g.ntiles + 1);
     size_t tmp_bytes = 0;
     SDF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys2, vals, vals2, total, 0, bits, st));
@@ -520,8 +564,11 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
   A.counters = ctx->d_counters;
   const int threads = g.t[0] * g.t[1] * g.t[2];
   if (g.ntiles > 0x7fffffffLL) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "grid has too many tiles");
-  k_tile_fold<<<(unsigned)g.ntiles, threads, 0, st>>>(A);
-  SDF_CUDA(ctx, cudaGetLastError());
+  SDF_MARK(ctx, T_TILES);
+  const size_t smem = sizeof(WarpStage) * (size_t)(threads / 32);
+  k_tile_fold<<<(unsigned)g.ntiles, threads, smem, st>>>(A);
+  SDF_KERNEL(ctx);
+  SDF_MARK(ctx, T_FOLD);
 
   if (mode == SDFGPU_MODE_REF_RULE) {
     // Can a node with an empty candidate set still have a triangle within h?  Only when some
@@ -535,7 +582,7 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
         SDF_CUDA(ctx, cudaMemsetAsync(band, 0, (size_t)g.ngp, st));
         const double hb = g.h * (1.0 + 1e-9) + (double)eD_abs + 2e-6 * g.E;
         k_band<<<grid_for(nel, 128), 128, 0, st>>>(v32, rec, nel, g, hb, (float)(hb * hb), band);
-        SDF_CUDA(ctx, cudaGetLastError());
+        SDF_KERNEL(ctx);
       }
       KnnArgs K;
       K.g = g;
@@ -555,7 +602,7 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
       K.xp = d_xp;
       K.counters = ctx->d_counters;
       k_knn_fallback<<<grid_for(g.ngp, 128, 148 * 16), 128, 0, st>>>(K);
-      SDF_CUDA(ctx, cudaGetLastError());
+      SDF_KERNEL(ctx);
     }
   }
   return 0;

@@ -229,6 +229,7 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
   if (!X || !IEN) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "X and IEN must not be NULL");
   ctx->has_mesh = false;
   ctx->mesh.ine_ready = false;
+  ctx->launches = 0;
   SDF_CUDA(ctx, cudaEventRecord(ctx->ev[4], st));
 
   double* dX;
@@ -257,9 +258,9 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
   SDF_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, sizeof(int64_t) * C_NUM, st));
   SDF_CUDA(ctx, cudaMemcpyAsync(bb, init, sizeof(init), cudaMemcpyHostToDevice, st));
   k_vertex_bbox<<<grid_for(nnp, 256, 148 * 8), 256, 0, st>>>(dX, nnp, bb);
-  SDF_CUDA(ctx, cudaGetLastError());
+  SDF_KERNEL(ctx);
   k_prep<<<grid_for(nel, 128), 128, 0, st>>>(dX, nnp, dIEN, nel, rec, cent, ctx->d_counters);
-  SDF_CUDA(ctx, cudaGetLastError());
+  SDF_KERNEL(ctx);
   unsigned long long hbb[8];
   int64_t hcnt[C_NUM];
   SDF_CUDA(ctx, cudaMemcpyAsync(hbb, bb, sizeof(hbb), cudaMemcpyDeviceToHost, st));
@@ -284,7 +285,7 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
   SDF_CUDA(ctx, cudaMemcpyAsync(bb + 7, &rho0, sizeof(rho0), cudaMemcpyHostToDevice, st));
   k_local32<<<grid_for(nel, 128), 128, 0, st>>>(rec, cent, nel, M.center[0], M.center[1], M.center[2], v32, c32,
                                                  box32, bb + 7);
-  SDF_CUDA(ctx, cudaGetLastError());
+  SDF_KERNEL(ctx);
 
   // LBVH
   const int n = (int)nel;
@@ -300,14 +301,14 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
   SDF_TRY(scratch_t(ctx, "leaf_prim", (size_t)n, &leaf_prim));
   if (n == 1) {
     k_single_root<<<1, 1, 0, st>>>(box32, nodes, leaf_prim);
-    SDF_CUDA(ctx, cudaGetLastError());
+    SDF_KERNEL(ctx);
   } else {
     const float lox = (float)(M.bmin[0] - M.center[0]), loy = (float)(M.bmin[1] - M.center[1]),
                 loz = (float)(M.bmin[2] - M.center[2]);
     const double ext = std::max(M.bmax[0] - M.bmin[0], std::max(M.bmax[1] - M.bmin[1], M.bmax[2] - M.bmin[2]));
     const float inv = ext > 0 ? (float)(1024.0 / ext) : 1.0f;
     k_morton<<<grid_for(nel, 256), 256, 0, st>>>(c32, nel, lox, loy, loz, inv, keys);
-    SDF_CUDA(ctx, cudaGetLastError());
+    SDF_KERNEL(ctx);
     size_t tmp_bytes = 0;
     SDF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, keys, keys2, n, 0, 62, st));
     void* tmp;
@@ -316,9 +317,9 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
     SDF_CUDA(ctx, cudaMemsetAsync(int_parent, 0xff, sizeof(int32_t) * n, st));
     SDF_CUDA(ctx, cudaMemsetAsync(flags, 0, sizeof(int32_t) * n, st));
     k_karras<<<grid_for(n - 1, 256), 256, 0, st>>>(keys2, n, nodes, int_parent, leaf_parent);
-    SDF_CUDA(ctx, cudaGetLastError());
+    SDF_KERNEL(ctx);
     k_refit<<<grid_for(n, 256), 256, 0, st>>>(keys2, box32, n, nodes, int_parent, leaf_parent, flags, leaf_prim);
-    SDF_CUDA(ctx, cudaGetLastError());
+    SDF_KERNEL(ctx);
   }
   unsigned long long hrho = 0;
   SDF_CUDA(ctx, cudaMemcpyAsync(&hrho, bb + 7, sizeof(hrho), cudaMemcpyDeviceToHost, st));
@@ -328,6 +329,7 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
   float ms = 0.f;
   SDF_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]));
   ctx->stats.ms_mesh = ms;
+  ctx->stats.mesh_launches = ctx->launches;
   ctx->stats.nel = nel;
   ctx->stats.rho_max = M.rho_max;
   ctx->has_mesh = true;
@@ -347,10 +349,10 @@ int ensure_ine(sdfgpu_ctx* ctx) {
   SDF_CUDA(ctx, cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (M.nnp + 1), st));
   SDF_CUDA(ctx, cudaMemsetAsync(cur, 0, sizeof(int32_t) * (M.nnp + 1), st));
   k_ine_count<<<grid_for(M.nel, 256), 256, 0, st>>>(dIEN, M.nel, cnt);
-  SDF_CUDA(ctx, cudaGetLastError());
+  SDF_KERNEL(ctx);
   SDF_TRY(cub_scan_i32(ctx, cnt, off, M.nnp + 1));
   k_ine_fill<<<grid_for(M.nel, 256), 256, 0, st>>>(dIEN, M.nel, off, cur, ine);
-  SDF_CUDA(ctx, cudaGetLastError());
+  SDF_KERNEL(ctx);
   M.ine_ready = true;
   return 0;
 }

@@ -117,7 +117,7 @@ __device__ __forceinline__ bool axis_range2(const GridP& g, int a, double x0, do
 template <int AX>
 __device__ __forceinline__ void tri_rows(const GridP& g, const TriRec64& r, bool fill, int64_t row_base,
                                          int32_t* row_cnt, const int32_t* row_off, int32_t* row_cur, RowHit* hits,
-                                         int64_t& nhit) {
+                                         unsigned long long* rkey, int32_t* ridx, int64_t& nhit) {
   const int b = AX == 0 ? 1 : 0, c = AX == 2 ? 1 : 2;
   int64_t b0, b1, c0, c1;
   if (!axis_range2(g, b, r.bmin[b], r.bmax[b], b0, b1)) return;
@@ -132,8 +132,13 @@ __device__ __forceinline__ void tri_rows(const GridP& g, const TriRec64& r, bool
       } else {
         RowHit R;
         if (row_test<AX>(r, ob, oc, &R)) {
-          const int32_t slot = atomicAdd(&row_cur[row], 1);
-          hits[row_off[row] + slot] = R;
+          const int32_t pos = row_off[row] + atomicAdd(&row_cur[row], 1);
+          hits[pos] = R;
+          // sort key: row in the high word, the hit coordinate (ordered float bits) in the low word
+          uint32_t u = __float_as_uint((float)R.key);
+          u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+          rkey[pos] = ((unsigned long long)row << 32) | u;
+          ridx[pos] = pos;
         }
       }
     }
@@ -142,13 +147,13 @@ __device__ __forceinline__ void tri_rows(const GridP& g, const TriRec64& r, bool
 
 __global__ void k_rows(const TriRec64* __restrict__ rec, int64_t nel, GridP g, int64_t base_y, int64_t base_z,
                        bool fill, int32_t* row_cnt, const int32_t* row_off, int32_t* row_cur, RowHit* hits,
-                       int64_t* counters) {
+                       unsigned long long* rkey, int32_t* ridx, int64_t* counters) {
   int64_t nhit = 0;
   for (int64_t el = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; el < nel; el += (int64_t)gridDim.x * blockDim.x) {
     const TriRec64 r = rec[el];
-    tri_rows<0>(g, r, fill, 0, row_cnt, row_off, row_cur, hits, nhit);
-    tri_rows<1>(g, r, fill, base_y, row_cnt, row_off, row_cur, hits, nhit);
-    tri_rows<2>(g, r, fill, base_z, row_cnt, row_off, row_cur, hits, nhit);
+    tri_rows<0>(g, r, fill, 0, row_cnt, row_off, row_cur, hits, rkey, ridx, nhit);
+    tri_rows<1>(g, r, fill, base_y, row_cnt, row_off, row_cur, hits, rkey, ridx, nhit);
+    tri_rows<2>(g, r, fill, base_z, row_cnt, row_off, row_cur, hits, rkey, ridx, nhit);
   }
   if (!fill) {
     for (int off = 16; off > 0; off >>= 1) nhit += __shfl_down_sync(0xffffffffu, nhit, off);
@@ -156,19 +161,11 @@ __global__ void k_rows(const TriRec64* __restrict__ rec, int64_t nel, GridP g, i
   }
 }
 
-// Orders each row's hits by their hit coordinate (insertion sort; rows are short).
-__global__ void k_sort_rows(int64_t nrows, const int32_t* __restrict__ row_off, const int32_t* __restrict__ row_cnt,
-                            RowHit* hits) {
-  for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < nrows; row += (int64_t)gridDim.x * blockDim.x) {
-    RowHit* h = hits + row_off[row];
-    const int n = row_cnt[row];
-    for (int a = 1; a < n; ++a) {
-      const RowHit v = h[a];
-      int b = a - 1;
-      while (b >= 0 && h[b].key > v.key) { h[b + 1] = h[b]; --b; }
-      h[b + 1] = v;
-    }
-  }
+// Gathers the row hits into (row, hit coordinate) order after the radix sort of their keys.
+__global__ void k_gather_rows(int64_t n, const int32_t* __restrict__ order, const RowHit* __restrict__ src,
+                              RowHit* __restrict__ dst) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    dst[q] = src[order[q]];
 }
 
 // Number of distinct hits (gaps > eps) among sorted t values passing the direction's t > eps.
@@ -485,31 +482,50 @@ int run_signs(sdfgpu_ctx* ctx, const GridP& g, int min_rays, int max_rays, doubl
   SDF_CUDA(ctx, cudaMemsetAsync(row_cnt, 0, sizeof(int32_t) * (nrows + 1), st));
   SDF_CUDA(ctx, cudaMemsetAsync(row_cur, 0, sizeof(int32_t) * (nrows + 1), st));
   k_rows<<<grid_for(nel, 128), 128, 0, st>>>(rec, nel, g, Rx, Rx + Ry, false, row_cnt, nullptr, nullptr, nullptr,
-                                             ctx->d_counters);
-  SDF_CUDA(ctx, cudaGetLastError());
+                                             nullptr, nullptr, ctx->d_counters);
+  SDF_KERNEL(ctx);
   SDF_TRY(cub_scan_i32(ctx, row_cnt, row_off, nrows + 1));
   int32_t total = 0;
   SDF_CUDA(ctx, cudaMemcpyAsync(&total, row_off + nrows, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   SDF_CUDA(ctx, cudaStreamSynchronize(st));
   if (total < 0) return fail(ctx, SDFGPU_ERR_CAPACITY, "more than 2^31 row hits");
-  RowHit* hits;
-  SDF_TRY(scratch_t(ctx, "row_hits", (size_t)std::max(total, 1), &hits));
+  RowHit *hits_raw, *hits;
+  unsigned long long *rkey, *rkey2;
+  int32_t *ridx, *ridx2;
+  const size_t H = (size_t)std::max(total, 1);
+  SDF_TRY(scratch_t(ctx, "row_hits_raw", H, &hits_raw));
+  SDF_TRY(scratch_t(ctx, "row_hits", H, &hits));
+  SDF_TRY(scratch_t(ctx, "row_key", H, &rkey));
+  SDF_TRY(scratch_t(ctx, "row_key2", H, &rkey2));
+  SDF_TRY(scratch_t(ctx, "row_idx", H, &ridx));
+  SDF_TRY(scratch_t(ctx, "row_idx2", H, &ridx2));
   if (total > 0) {
-    k_rows<<<grid_for(nel, 128), 128, 0, st>>>(rec, nel, g, Rx, Rx + Ry, true, nullptr, row_off, row_cur, hits,
-                                               ctx->d_counters);
-    SDF_CUDA(ctx, cudaGetLastError());
-    k_sort_rows<<<grid_for(nrows, 128), 128, 0, st>>>(nrows, row_off, row_cnt, hits);
-    SDF_CUDA(ctx, cudaGetLastError());
+    k_rows<<<grid_for(nel, 128), 128, 0, st>>>(rec, nel, g, Rx, Rx + Ry, true, nullptr, row_off, row_cur, hits_raw,
+                                               rkey, ridx, ctx->d_counters);
+    SDF_KERNEL(ctx);
+    int bits = 32;
+    while (bits < 64 && (1LL << (bits - 32)) < nrows) ++bits;
+    size_t tmp_bytes = 0;
+    SDF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, rkey, rkey2, ridx, ridx2, total, 0, bits, st));
+    void* tmp;
+    SDF_TRY(scratch(ctx, "cub_tmp", tmp_bytes, &tmp));
+    SDF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, rkey, rkey2, ridx, ridx2, total, 0, bits, st));
+    k_gather_rows<<<grid_for(total, 256), 256, 0, st>>>(total, ridx2, hits_raw, hits);
+    SDF_KERNEL(ctx);
   }
   uint8_t *px, *py, *pz;
   SDF_TRY(scratch_t(ctx, "par_x", (size_t)g.ngp, &px));
   SDF_TRY(scratch_t(ctx, "par_y", (size_t)g.ngp, &py));
   SDF_TRY(scratch_t(ctx, "par_z", (size_t)g.ngp, &pz));
   const unsigned gp = grid_for(g.ngp, 256, 148 * 16);
+  SDF_MARK(ctx, T_ROWS);
   k_axis_parity<0><<<gp, 256, 0, st>>>(g, 0, row_off, row_cnt, hits, px);
+  SDF_KERNEL(ctx);
   k_axis_parity<1><<<gp, 256, 0, st>>>(g, Rx, row_off, row_cnt, hits, py);
+  SDF_KERNEL(ctx);
   k_axis_parity<2><<<gp, 256, 0, st>>>(g, Rx + Ry, row_off, row_cnt, hits, pz);
-  SDF_CUDA(ctx, cudaGetLastError());
+  SDF_KERNEL(ctx);
+  SDF_MARK(ctx, T_PARITY);
 
   int32_t *und, *wind;
   SDF_TRY(scratch_t(ctx, "und_list", (size_t)g.ngp, &und));
@@ -527,7 +543,7 @@ int run_signs(sdfgpu_ctx* ctx, const GridP& g, int min_rays, int max_rays, doubl
   V.wind_list = wind;
   V.counters = ctx->d_counters;
   k_vote<<<grid_for(g.ngp, 256, 148 * 16), 256, 0, st>>>(V);
-  SDF_CUDA(ctx, cudaGetLastError());
+  SDF_KERNEL(ctx);
 
   RayArgs R;
   R.g = g;
@@ -547,14 +563,14 @@ int run_signs(sdfgpu_ctx* ctx, const GridP& g, int min_rays, int max_rays, doubl
   R.wind_list = wind;
   R.counters = ctx->d_counters;
   k_adaptive<<<148 * 8, 128, 0, st>>>(R);
-  SDF_CUDA(ctx, cudaGetLastError());
+  SDF_KERNEL(ctx);
   if (use_winding) {
     k_winding<<<148 * 4, 256, 0, st>>>(g, rec, nel, wind, d_sign, ctx->d_counters);
-    SDF_CUDA(ctx, cudaGetLastError());
+    SDF_KERNEL(ctx);
   }
   if (d_sdf && d_dist) {
     k_combine<<<grid_for(g.ngp, 256, 148 * 16), 256, 0, st>>>(g.ngp, d_dist, d_sign, d_sdf);
-    SDF_CUDA(ctx, cudaGetLastError());
+    SDF_KERNEL(ctx);
   }
   return 0;
 }

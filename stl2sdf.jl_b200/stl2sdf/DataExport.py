@@ -28,7 +28,8 @@ def exportSdfToVTI(filename: str, grid, values, value_label: str, smooth=None, c
     values = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
     if values.shape[0] != int(np.prod(dims)):
         raise ValueError(f"Values vector length ({values.shape[0]}) doesn't match grid dimensions ({int(np.prod(dims))}).")
-    o = np.asarray(grid.AABB_min, dtype=np.float64)
+    o = [float(v) for v in np.asarray(grid.AABB_min, dtype=np.float64)]
+    h = float(h)
     ext = f"0 {dims[0] - 1} 0 {dims[1] - 1} 0 {dims[2] - 1}"
     raw = values.astype("<f8").tobytes()
     if compress:

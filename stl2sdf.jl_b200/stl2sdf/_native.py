@@ -46,6 +46,9 @@ class Stats(ctypes.Structure):
         ("undecided_nodes", ctypes.c_int64), ("extra_rays", ctypes.c_int64), ("winding_nodes", ctypes.c_int64),
         ("winding_ambiguous", ctypes.c_int64), ("unbounded_fallbacks", ctypes.c_int64), ("rho_max", ctypes.c_double),
         ("ms_distance", ctypes.c_double), ("ms_sign", ctypes.c_double), ("ms_mesh", ctypes.c_double),
+        ("launches", ctypes.c_int64), ("mesh_launches", ctypes.c_int64), ("ms_tiles", ctypes.c_double),
+        ("ms_fold", ctypes.c_double), ("ms_rows", ctypes.c_double), ("ms_parity", ctypes.c_double),
+        ("ms_vote", ctypes.c_double),
     ]
 
     def as_dict(self):

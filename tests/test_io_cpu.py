@@ -1,0 +1,129 @@
+"""Data formats either side of the hot path: STL import/dedupe (ImportStlData.jl), VTI export
+(ExportToVTI.jl), the synthetic workload meshes and the Python mirror of MeshGrid."""
+
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import GOLDEN
+
+
+def test_reference_fixture_import():
+    """The reference's own test input: 3,712 triangles, 1,890 unique vertices, closed."""
+    from stl2sdf import DataImport, synthetic
+
+    X, IEN = DataImport.import_stl(os.path.join(GOLDEN, "artifacts.stl"))
+    assert IEN.shape == (3712, 3) and X.shape == (1890, 3)
+    assert synthetic.is_closed(IEN)
+    assert IEN.min() == 1 and IEN.max() == X.shape[0]
+
+
+def test_binary_roundtrip_and_first_appearance_order(tmp_path):
+    from stl2sdf import DataImport, synthetic
+
+    V, F = synthetic.icosphere(2, jitter=0.01, seed=3)
+    path = str(tmp_path / "s.stl")
+    DataImport.write_binary_stl(path, V, F)
+    X, IEN = DataImport.import_stl(path)
+    X2, IEN2 = DataImport.roundtrip_float32(V, F)
+    assert np.array_equal(X, X2) and np.array_equal(IEN, IEN2)
+    # vertices appear in the order the triangle stream first mentions them
+    first = np.unique(IEN.reshape(-1), return_index=True)[1]
+    assert np.all(np.diff(first) > 0)
+    assert np.array_equal(X, V[F.reshape(-1)[np.sort(np.unique(F.reshape(-1), return_index=True)[1])] - 1]
+                          .astype(np.float32).astype(np.float64))
+
+
+def test_ascii_reader(tmp_path):
+    from stl2sdf import DataImport
+
+    path = str(tmp_path / "a.stl")
+    with open(path, "w") as f:
+        f.write("solid t\n facet normal 0 0 1\n  outer loop\n   vertex 0 0 0\n   vertex 1 0 0\n   vertex 0 1 0\n"
+                "  endloop\n endfacet\n facet normal 0 0 1\n  outer loop\n   vertex 1 0 0\n   vertex 1 1 0\n"
+                "   vertex 0 1 0\n  endloop\n endfacet\nendsolid t\n")
+    X, IEN = DataImport.import_stl(path)
+    assert X.shape == (4, 3) and IEN.tolist() == [[1, 2, 3], [2, 4, 3]]
+
+
+def test_dedupe_tolerance_path_matches_sequential():
+    from stl2sdf import DataImport
+
+    V = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [1e-11, 0, 0], [1, 1, 0], [0, 1, 0]], dtype=np.float64)
+    T = np.array([[1, 2, 3], [4, 5, 6]])
+    X, IEN = DataImport.process_stl_mesh(V, T)
+    Xs, IENs = DataImport._dedupe_sequential(V, T)
+    assert np.array_equal(X, Xs) and np.array_equal(IEN, IENs)
+    assert X.shape[0] == 4 and IEN[1, 0] == 1  # 1e-11 merged into the origin
+
+
+def test_vti_roundtrip(tmp_path):
+    from stl2sdf import DataExport, MeshGrid
+
+    g = MeshGrid.Grid([0.0, 0.0, 0.0], [1.0, 0.5, 0.25], 8, 3)
+    vals = np.random.default_rng(0).normal(size=g.ngp)
+    for comp in (True, False):
+        path = DataExport.exportSdfToVTI(str(tmp_path / f"x{comp}_sdf"), g, vals, "distance", compress=comp)
+        assert path.endswith(".vti")
+        v, dims, o, sp, label = DataExport.read_vti(path)
+        assert np.array_equal(v, vals) and dims.tolist() == (g.N + 1).tolist()
+        assert np.array_equal(o, g.AABB_min) and sp.tolist() == [g.cell_size] * 3 and label == "distance"
+    with pytest.raises(ValueError):
+        DataExport.exportSdfToVTI(str(tmp_path / "bad"), g, vals[:-1], "distance")
+
+
+def test_workload_meshes():
+    from stl2sdf import synthetic
+
+    V, F = synthetic.icosphere(4)
+    assert V.shape == (2562, 3) and F.shape == (5120, 3) and synthetic.is_closed(F)
+    V, F = synthetic.torus()
+    assert V.shape == (65536, 3) and F.shape == (131072, 3) and synthetic.is_closed(F)
+    V, F = synthetic.box()
+    assert F.shape == (12, 3) and synthetic.is_closed(F)
+
+
+def test_grid_points_match_oracle_nodes(icosphere_mesh):
+    from stl2sdf import MeshGrid
+
+    X, IEN = icosphere_mesh
+    mesh = MeshGrid.TriangularMesh(X, IEN)
+    g = MeshGrid.noninteractive_sdf_grid_setup(mesh, 0.05)
+    P = MeshGrid.generateGridPoints(g)
+    assert P.shape == (3, g.ngp)
+    n = g.N + 1
+    for lin in (0, 1, n[0], n[0] * n[1] + 5, g.ngp - 1):
+        i, j, k = lin % n[0], (lin // n[0]) % n[1], lin // (n[0] * n[1])
+        assert P[:, lin].tolist() == [g.AABB_min[0] + g.cell_size * i, g.AABB_min[1] + g.cell_size * j,
+                                      g.AABB_min[2] + g.cell_size * k]
+    xmin, xmax = MeshGrid.getMesh_AABB(mesh.X)
+    assert np.array_equal(xmin, X.min(0)) and np.array_equal(xmax, X.max(0))
+    assert len(mesh.INE) == mesh.nnp and sum(len(v) for v in mesh.INE) == 3 * mesh.nel
+
+
+def test_artifact_removal():
+    from stl2sdf import MeshGrid, remove_sdf_artifacts, analyze_sdf_components
+
+    g = MeshGrid.Grid.from_parts([0.0, 0.0, 0.0], [19, 19, 19], 0.1)
+    n = g.N + 1
+    sdf = -np.ones(g.ngp)
+    vol = sdf.reshape(n[2], n[1], n[0])
+    vol[2:12, 2:12, 2:12] = 1.0   # large interior component (1000 nodes)
+    vol[15:17, 15:17, 15:16] = 1.0  # small one (4 nodes)
+    comps = analyze_sdf_components(sdf, g)
+    assert sorted(comps.values()) == [4, 1000]
+    flipped = remove_sdf_artifacts(sdf, g, min_component_ratio=0.01)
+    assert flipped == 4 and np.count_nonzero(sdf > 0) == 1000
+
+
+def test_options_validation():
+    import stl2sdf
+
+    with pytest.raises(AssertionError):
+        stl2sdf.stl_to_sdf("x.stl", stl2sdf.Options(grid_refinement=3))
+    with pytest.raises(AssertionError):
+        stl2sdf.stl_to_sdf("x.stl", stl2sdf.Options(artifact_ratio=1.5))
