@@ -47,6 +47,18 @@ def make_workload(name: str):
         X, IEN = DataImport.roundtrip_float32(V, F)
         o, amax, N, h, ngp = _native.grid_setup(X.min(0), X.max(0), 128 - 7, 3)
         desc = "torus R=1 r=0.3 512x128 quads (131072 tris) noise U(-2%,2%) seed 1, 128 nodes on the long axis"
+    elif name == "blobs256":
+        V, F = synthetic.blobs(64, seed=2, cells=512)
+        X, IEN = DataImport.roundtrip_float32(V, F)
+        o, amax, N, h, ngp = _native.grid_setup(X.min(0), X.max(0), 256 - 7, 3)
+        desc = (f"marching cubes (512^3) of the 0.5 level of 64 Gaussian blobs (centres U[-1,1]^3, sigma U[0.1,0.3], "
+                f"seed 2): {IEN.shape[0]} tris, 256 nodes on the long axis")
+    elif name == "gyroid320":
+        V, F = synthetic.gyroid(384, 0.04, 2.0)
+        X, IEN = DataImport.roundtrip_float32(V, F)
+        o, amax, N, h, ngp = _native.grid_setup(X.min(0), X.max(0), 320 - 7, 3)
+        desc = (f"marching cubes (384^3) of the gyroid sheet |g| <= 0.04 over [0,4pi]^3 with an outside border: "
+                f"{IEN.shape[0]} tris, 320 nodes on the long axis")
     else:
         raise SystemExit(f"unknown workload {name}")
     g = dict(origin=np.asarray(o), N=np.asarray(N), h=float(h), ngp=int(ngp))

@@ -145,6 +145,7 @@ struct FoldArgs {
 struct __align__(16) WarpStage {
   float4 v[32][3];
   float4 c[32];
+  float4 lo[32], hi[32];  // FP32 box of the entry
   int32_t id[32];
   float D[32][32];  // [entry][lane]
 };
@@ -183,11 +184,14 @@ __global__ void __launch_bounds__(256) k_tile_fold(FoldArgs A) {
       S.v[lane][1] = __ldg(&A.v32[3 * tri + 1]);
       S.v[lane][2] = __ldg(&A.v32[3 * tri + 2]);
       S.c[lane] = __ldg(&A.c32[tri]);
+      const float4 a = S.v[lane][0], b = S.v[lane][1], c = S.v[lane][2];
+      S.lo[lane] = make_float4(fminf(a.x, fminf(b.x, c.x)), fminf(a.y, fminf(b.y, c.y)), fminf(a.z, fminf(b.z, c.z)), 0.f);
+      S.hi[lane] = make_float4(fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y)), fmaxf(a.z, fmaxf(b.z, c.z)), 0.f);
     }
     __syncwarp();
     uint32_t bits = 0;
     if (valid) {
-      const float lim = have ? (float)m + A.eD_abs + A.eD_rel * (float)m : 3.0e38f;
+      const float lim = have ? (float)m + A.eD_abs + A.eD_rel * (float)m : 1.0e18f;
       for (int q = 0; q < nE; ++q) {
         if (ref) {
           const float4 c = S.c[q];
@@ -204,6 +208,9 @@ __global__ void __launch_bounds__(256) k_tile_fold(FoldArgs A) {
           }
         }
         any = true;
+        // box reject (the reference's point_in_box_range against the running minimum, with the
+        // FP32 margin): a triangle whose box is farther than m cannot change the fold
+        if (box_d2(p32, f3(S.lo[q]), f3(S.hi[q])) > lim * lim) continue;
         const float D = sqrtf(pt_tri_d2(p32, f3(S.v[q][0]), f3(S.v[q][1]), f3(S.v[q][2])));
         if (D <= lim) {
           bits |= 1u << q;

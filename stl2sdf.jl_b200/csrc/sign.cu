@@ -279,6 +279,8 @@ struct VoteArgs {
   double* sign;
   double* conf;
   int32_t* und_list;
+  uint64_t* und_have;
+  uint64_t* und_par;
   int32_t* wind_list;
   int64_t* counters;
 };
@@ -295,6 +297,13 @@ __global__ void k_vote(VoteArgs A) {
     if (rc) {
       const int64_t slot = atomicAdd((unsigned long long*)&A.counters[C_LIST_UNDECIDED], 1ULL);
       A.und_list[slot] = (int32_t)lin;
+      uint64_t have = 0, par = 0;
+      if (!ovf) {
+        have = 0x3FULL;
+        for (int r = 1; r <= 6; ++r) par |= (uint64_t)axis_bit(px, py, pz, r) << (r - 1);
+      }
+      A.und_have[slot] = have;
+      A.und_par[slot] = par;
       continue;
     }
     if (A.use_winding && cf < A.conf_thresh) {
@@ -323,6 +332,14 @@ struct RayArgs {
   double* conf;
   int32_t* wind_list;
   int64_t* counters;
+  uint64_t* have;     // per undecided node: rays whose parity is known
+  uint64_t* parbits;  // per undecided node: their parities
+  uint8_t* done;
+  int32_t* req_node;  // requests of the current round
+  int8_t* req_ray;
+  int64_t* rq_cnt;    // requests per round
+  int speculative;    // request all remaining rays at once (latency-bound when few nodes remain)
+  int last_ray;       // last ray index the vote can cast: min(36, max(min_rays, max_rays))
 };
 
 __device__ __forceinline__ void child_box2(const BNode& nd, int side, float3& lo, float3& hi) {
@@ -378,30 +395,64 @@ __device__ int ray_parity(const RayArgs& A, const d3& p, const float3& p32, int 
   return unique & 1;
 }
 
-__global__ void __launch_bounds__(128) k_adaptive(RayArgs A) {
+// The reference's vote (:234-288) replayed over the rays whose parity is already known (bit i-1
+// of `have` / `par` for ray i).  Returns 0 with sign/conf when the vote is decided; otherwise 1
+// with [need_lo, need_hi] = the rays of the first incomplete step (the initial min_rays, or the
+// current batch of 4), which the caller requests all at once.
+__device__ __forceinline__ int vote_known(uint64_t have, uint64_t par, int min_rays, int max_rays, double& sign,
+                                          double& conf, int& need_lo, int& need_hi) {
+  int inside = 0, total = 0;
+  for (int i = 1; i <= min_rays; ++i) {
+    if (!((have >> (i - 1)) & 1)) { need_lo = i; need_hi = min_rays; return 1; }
+    inside += (int)((par >> (i - 1)) & 1);
+    ++total;
+  }
+  double ratio = dd((double)inside, (double)total);
+  double cf = fmax(ratio, ds(1.0, ratio));
+  int used = min_rays;
+  while (cf < 0.85 && used < max_rays) {
+    const int batch = min(4, max_rays - used);
+    for (int i = used + 1; i <= used + batch; ++i) {
+      if (i <= 36) {
+        if (!((have >> (i - 1)) & 1)) { need_lo = i; need_hi = min(used + batch, 36); return 1; }
+        inside += (int)((par >> (i - 1)) & 1);
+        ++total;
+      }
+    }
+    used += batch;
+    ratio = dd((double)inside, (double)total);
+    cf = fmax(ratio, ds(1.0, ratio));
+    if (cf > 0.95) break;
+  }
+  sign = ratio > 0.5 ? 1.0 : -1.0;
+  conf = cf;
+  return 0;
+}
+
+// One round of the adaptive vote over the undecided nodes: decide, or request the next rays.
+__global__ void k_round(RayArgs A, int64_t nund, int round, int last) {
   const GridP& g = A.g;
-  const int64_t count = A.counters[C_LIST_UNDECIDED];
-  int64_t rays = 0;
-  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < count; q += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t lin = A.list[q];
-    const int64_t i = lin % g.n[0], j = (lin / g.n[0]) % g.n[1], k = lin / (g.n[0] * g.n[1]);
-    const d3 p = node_coord(g.o, g.h, i, j, k);
-    const float3 p32 = make_float3((float)(p.x - g.center[0]), (float)(p.y - g.center[1]), (float)(p.z - g.center[2]));
-    const uint8_t px = A.par[0][lin], py = A.par[1][lin], pz = A.par[2][lin];
-    const bool ovf = ((px | py | pz) & 0x80) != 0;
-    bool bad = false;
+  int64_t* rq_cnt = A.rq_cnt + round;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nund; q += (int64_t)gridDim.x * blockDim.x) {
+    if (A.done[q]) continue;
     double s, cf;
-    int total;
-    vote_logic(A.min_rays, A.max_rays,
-               [&](int r) {
-                 if (r <= 6 && !ovf) return axis_bit(px, py, pz, r);
-                 ++rays;
-                 const int v = ray_parity(A, p, p32, r - 1);
-                 if (v < 0) { bad = true; return 0; }
-                 return v;
-               },
-               s, cf, total);
-    if (bad) count_add(A.counters, C_ERR_CAPACITY, 1);
+    int lo, hi;
+    const uint64_t have = A.have[q], par = A.parbits[q];
+    if (vote_known(have, par, A.min_rays, A.max_rays, s, cf, lo, hi)) {
+      if (last) {  // unreachable: the rounds cover every batch up to the 36th direction
+        count_add(A.counters, C_ERR_CAPACITY, 1);
+        continue;
+      }
+      if (A.speculative) hi = A.last_ray;  // few nodes: cast every ray the vote could still need
+      for (int i = lo; i <= hi; ++i) {
+        if ((have >> (i - 1)) & 1) continue;
+        const int64_t slot = atomicAdd((unsigned long long*)rq_cnt, 1ULL);
+        A.req_node[slot] = (int32_t)q;
+        A.req_ray[slot] = (int8_t)i;
+      }
+      continue;
+    }
+    const int64_t lin = A.list[q];
     if (A.use_winding && cf < A.conf_thresh) {
       const int64_t slot = atomicAdd((unsigned long long*)&A.counters[C_LIST_WINDING], 1ULL);
       A.wind_list[slot] = (int32_t)lin;
@@ -409,22 +460,51 @@ __global__ void __launch_bounds__(128) k_adaptive(RayArgs A) {
     }
     A.sign[lin] = s;
     if (A.conf) A.conf[lin] = cf;
+    A.done[q] = 1;
+    (void)g;
+  }
+}
+
+// Casts the requested rays of a round, one thread per (node, ray).
+__global__ void __launch_bounds__(128) k_rays(RayArgs A, int round) {
+  const GridP& g = A.g;
+  const int64_t count = A.rq_cnt[round];
+  int64_t rays = 0;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t q = A.req_node[t];
+    const int r = A.req_ray[t];
+    const int64_t lin = A.list[q];
+    const int64_t i = lin % g.n[0], j = (lin / g.n[0]) % g.n[1], k = lin / (g.n[0] * g.n[1]);
+    const d3 p = node_coord(g.o, g.h, i, j, k);
+    const float3 p32 = make_float3((float)(p.x - g.center[0]), (float)(p.y - g.center[1]), (float)(p.z - g.center[2]));
+    int v = ray_parity(A, p, p32, r - 1);
+    if (v < 0) { count_add(A.counters, C_ERR_CAPACITY, 1); v = 0; }
+    const uint64_t bit = 1ULL << (r - 1);
+    if (v) atomicOr((unsigned long long*)&A.parbits[q], (unsigned long long)bit);
+    atomicOr((unsigned long long*)&A.have[q], (unsigned long long)bit);
+    ++rays;
   }
   for (int off = 16; off > 0; off >>= 1) rays += __shfl_down_sync(0xffffffffu, rays, off);
   if ((threadIdx.x & 31) == 0 && rays) count_add(A.counters, C_EXTRA_RAYS, rays);
 }
 
-// generalized_winding_number (:295-328): one CTA per node, fixed-order block reduction.
+// generalized_winding_number (:295-328).  The triangles are cut into fixed chunks; one CTA sums
+// one chunk for one node (fixed-order block reduction) and k_winding_final adds the chunk sums
+// in chunk order, so the result does not depend on scheduling and one node still fills the GPU.
+constexpr int kWindChunk = 8192;
+
 __global__ void __launch_bounds__(256) k_winding(GridP g, const TriRec64* __restrict__ rec, int64_t nel,
-                                                 const int32_t* __restrict__ list, double* sign, int64_t* counters) {
+                                                 const int32_t* __restrict__ list, int64_t count, int nchunks,
+                                                 double* __restrict__ partial) {
   __shared__ double red[256];
-  const int64_t count = counters[C_LIST_WINDING];
-  for (int64_t q = blockIdx.x; q < count; q += gridDim.x) {
+  const int chunk = blockIdx.x;
+  for (int64_t q = blockIdx.y; q < count; q += gridDim.y) {
     const int64_t lin = list[q];
     const int64_t i = lin % g.n[0], j = (lin / g.n[0]) % g.n[1], k = lin / (g.n[0] * g.n[1]);
     const d3 p = node_coord(g.o, g.h, i, j, k);
     double w = 0.0;
-    for (int64_t el = threadIdx.x; el < nel; el += blockDim.x) {
+    const int64_t e1 = min((int64_t)(chunk + 1) * kWindChunk, nel);
+    for (int64_t el = (int64_t)chunk * kWindChunk + threadIdx.x; el < e1; el += blockDim.x) {
       const TriRec64& r = rec[el];
       const d3 a = v_normalize(v_sub(rec_v(r, 0), p));
       const d3 b = v_normalize(v_sub(rec_v(r, 1), p));
@@ -439,17 +519,24 @@ __global__ void __launch_bounds__(256) k_winding(GridP g, const TriRec64* __rest
     }
     red[threadIdx.x] = w;
     __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-      if ((int)threadIdx.x < s) red[threadIdx.x] = da(red[threadIdx.x], red[threadIdx.x + s]);
+    for (int s2 = blockDim.x / 2; s2 > 0; s2 >>= 1) {
+      if ((int)threadIdx.x < s2) red[threadIdx.x] = da(red[threadIdx.x], red[threadIdx.x + s2]);
       __syncthreads();
     }
-    if (threadIdx.x == 0) {
-      const double wn = dd(red[0], 12.566370614359172);  // 4π
-      sign[lin] = fabs(wn) > 0.5 ? 1.0 : -1.0;
-      count_add(counters, C_WINDING, 1);
-      if (fabs(fabs(wn) - 0.5) < 1e-9) count_add(counters, C_WIND_AMBIG, 1);
-    }
+    if (threadIdx.x == 0) partial[q * nchunks + chunk] = red[0];
     __syncthreads();
+  }
+}
+
+__global__ void k_winding_final(const int32_t* __restrict__ list, int64_t count, int nchunks,
+                                const double* __restrict__ partial, double* sign, int64_t* counters) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < count; q += (int64_t)gridDim.x * blockDim.x) {
+    double w = 0.0;
+    for (int c = 0; c < nchunks; ++c) w = da(w, partial[q * nchunks + c]);
+    const double wn = dd(w, 12.566370614359172);  // 4π
+    sign[list[q]] = fabs(wn) > 0.5 ? 1.0 : -1.0;
+    count_add(counters, C_WINDING, 1);
+    if (fabs(fabs(wn) - 0.5) < 1e-9) count_add(counters, C_WIND_AMBIG, 1);
   }
 }
 
@@ -528,7 +615,10 @@ int run_signs(sdfgpu_ctx* ctx, const GridP& g, int min_rays, int max_rays, doubl
   SDF_MARK(ctx, T_PARITY);
 
   int32_t *und, *wind;
+  uint64_t *und_have, *und_par;
   SDF_TRY(scratch_t(ctx, "und_list", (size_t)g.ngp, &und));
+  SDF_TRY(scratch_t(ctx, "und_have", (size_t)g.ngp, &und_have));
+  SDF_TRY(scratch_t(ctx, "und_par", (size_t)g.ngp, &und_par));
   SDF_TRY(scratch_t(ctx, "wind_list", (size_t)g.ngp, &wind));
   VoteArgs V;
   V.g = g;
@@ -540,33 +630,77 @@ int run_signs(sdfgpu_ctx* ctx, const GridP& g, int min_rays, int max_rays, doubl
   V.sign = d_sign;
   V.conf = d_conf;
   V.und_list = und;
+  V.und_have = und_have;
+  V.und_par = und_par;
   V.wind_list = wind;
   V.counters = ctx->d_counters;
   k_vote<<<grid_for(g.ngp, 256, 148 * 16), 256, 0, st>>>(V);
   SDF_KERNEL(ctx);
-
-  RayArgs R;
-  R.g = g;
-  R.nodes = buf<BNode>(ctx, "nodes");
-  R.leaf_prim = buf<int32_t>(ctx, "leaf_prim");
-  R.rec = rec;
-  R.pad = (float)(2e-6 * g.E);
-  R.max_visits = 2 * nel + 64;
-  R.par[0] = px; R.par[1] = py; R.par[2] = pz;
-  R.list = und;
-  R.min_rays = min_rays;
-  R.max_rays = max_rays;
-  R.conf_thresh = conf_thresh;
-  R.use_winding = use_winding;
-  R.sign = d_sign;
-  R.conf = d_conf;
-  R.wind_list = wind;
-  R.counters = ctx->d_counters;
-  k_adaptive<<<148 * 8, 128, 0, st>>>(R);
-  SDF_KERNEL(ctx);
-  if (use_winding) {
-    k_winding<<<148 * 4, 256, 0, st>>>(g, rec, nel, wind, d_sign, ctx->d_counters);
+  int64_t nund = 0;
+  SDF_CUDA(ctx, cudaMemcpyAsync(&nund, ctx->d_counters + C_LIST_UNDECIDED, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  SDF_CUDA(ctx, cudaStreamSynchronize(st));
+  if (nund > 0) {
+    // Rounds of the adaptive vote: decide what is decidable, cast the next requested rays.
+    constexpr int kRounds = 12;  // initial rays + at most 8 batches reach the 36 directions
+    uint8_t* done;
+    int32_t* req_node;
+    int8_t* req_ray;
+    int64_t* rq_cnt;
+    SDF_TRY(scratch_t(ctx, "und_done", (size_t)nund, &done));
+    SDF_TRY(scratch_t(ctx, "req_node", (size_t)nund * 36, &req_node));
+    SDF_TRY(scratch_t(ctx, "req_ray", (size_t)nund * 36, &req_ray));
+    SDF_TRY(scratch_t(ctx, "rq_cnt", (size_t)kRounds + 1, &rq_cnt));
+    SDF_CUDA(ctx, cudaMemsetAsync(done, 0, (size_t)nund, st));
+    SDF_CUDA(ctx, cudaMemsetAsync(rq_cnt, 0, sizeof(int64_t) * (kRounds + 1), st));
+    RayArgs R;
+    R.g = g;
+    R.nodes = buf<BNode>(ctx, "nodes");
+    R.leaf_prim = buf<int32_t>(ctx, "leaf_prim");
+    R.rec = rec;
+    R.pad = (float)(2e-6 * g.E);
+    R.max_visits = 2 * nel + 64;
+    R.par[0] = px; R.par[1] = py; R.par[2] = pz;
+    R.list = und;
+    R.min_rays = min_rays;
+    R.max_rays = max_rays;
+    R.conf_thresh = conf_thresh;
+    R.use_winding = use_winding;
+    R.sign = d_sign;
+    R.conf = d_conf;
+    R.wind_list = wind;
+    R.counters = ctx->d_counters;
+    R.have = und_have;
+    R.parbits = und_par;
+    R.done = done;
+    R.req_node = req_node;
+    R.req_ray = req_ray;
+    R.rq_cnt = rq_cnt;
+    R.speculative = nund <= 8192;
+    R.last_ray = std::min(36, std::max(min_rays, max_rays));
+    const int rounds = R.speculative ? 1 : kRounds;
+    for (int r = 0; r < rounds; ++r) {
+      k_round<<<grid_for(nund, 128), 128, 0, st>>>(R, nund, r, 0);
+      SDF_KERNEL(ctx);
+      k_rays<<<grid_for(nund * 8, 128, 148 * 32), 128, 0, st>>>(R, r);
+      SDF_KERNEL(ctx);
+    }
+    k_round<<<grid_for(nund, 128), 128, 0, st>>>(R, nund, kRounds, 1);
     SDF_KERNEL(ctx);
+  }
+  if (use_winding) {
+    int64_t nw = 0;
+    SDF_CUDA(ctx, cudaMemcpyAsync(&nw, ctx->d_counters + C_LIST_WINDING, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    SDF_CUDA(ctx, cudaStreamSynchronize(st));
+    if (nw > 0) {
+      const int nchunks = (int)cdiv(nel, kWindChunk);
+      double* partial;
+      SDF_TRY(scratch_t(ctx, "wind_partial", (size_t)nw * nchunks, &partial));
+      dim3 grid((unsigned)nchunks, (unsigned)std::min<int64_t>(nw, 65535));
+      k_winding<<<grid, 256, 0, st>>>(g, rec, nel, wind, nw, nchunks, partial);
+      SDF_KERNEL(ctx);
+      k_winding_final<<<grid_for(nw, 128), 128, 0, st>>>(wind, nw, nchunks, partial, d_sign, ctx->d_counters);
+      SDF_KERNEL(ctx);
+    }
   }
   if (d_sdf && d_dist) {
     k_combine<<<grid_for(g.ngp, 256, 148 * 16), 256, 0, st>>>(g.ngp, d_dist, d_sign, d_sdf);

@@ -116,6 +116,98 @@ def box(lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0)):
     return V, F + 1
 
 
+_MG = None
+
+
+def _meshgen():
+    global _MG
+    if _MG is None:
+        import ctypes
+        import os
+
+        path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "lib", "libmeshgen.so")
+        L = ctypes.CDLL(os.path.abspath(path))
+        dp, i64p = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)
+        L.mg_blobs.argtypes = [dp, dp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.mg_blobs.restype = ctypes.c_void_p
+        L.mg_gyroid.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.mg_gyroid.restype = ctypes.c_void_p
+        L.mg_sizes.argtypes = [ctypes.c_void_p, i64p, i64p]
+        L.mg_copy.argtypes = [ctypes.c_void_p, dp, i64p]
+        L.mg_free.argtypes = [ctypes.c_void_p]
+        L.mg_table.argtypes = [ctypes.POINTER(ctypes.c_int8), ctypes.POINTER(ctypes.c_int32)]
+        _MG = L
+    return _MG
+
+
+def _collect(h):
+    import ctypes
+
+    L = _meshgen()
+    nv, nt = ctypes.c_int64(), ctypes.c_int64()
+    L.mg_sizes(h, ctypes.byref(nv), ctypes.byref(nt))
+    V = np.empty((nv.value, 3)); T = np.empty((nt.value, 3), dtype=np.int64)
+    L.mg_copy(h, V.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), T.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+    L.mg_free(h)
+    return V, T
+
+
+def blob_params(nblobs: int = 64, seed: int = 2, lo_sigma: float = 0.1, hi_sigma: float = 0.3):
+    """Centres U[-1,1]^3 and sigmas U[lo,hi] from numpy's default_rng(seed)."""
+    rng = np.random.default_rng(seed)
+    centers = rng.uniform(-1.0, 1.0, size=(nblobs, 3))
+    sigmas = rng.uniform(lo_sigma, hi_sigma, size=nblobs)
+    return centers, sigmas
+
+
+def blobs(nblobs: int = 64, seed: int = 2, cells: int = 512, iso: float = 0.5, box: float = 2.0):
+    """Marching-cubes surface of the iso level of a sum of unit-amplitude Gaussian blobs.
+
+    The lattice spans [-box, box]^3 with `cells` cells per axis; at distance >= 1 from every
+    centre each blob is below exp(-1/0.18) < 0.004, so the field stays below 0.5 on the border
+    of the default box and the surface is closed.  64 blobs at 512^3 give about 1.5M triangles.
+    """
+    import ctypes
+
+    c, s = blob_params(nblobs, seed)
+    c = np.ascontiguousarray(c); s = np.ascontiguousarray(s)
+    dp = ctypes.POINTER(ctypes.c_double)
+    h = _meshgen().mg_blobs(c.ctypes.data_as(dp), s.ctypes.data_as(dp), nblobs, iso, cells + 1, -box, box)
+    return _collect(h)
+
+
+def gyroid(cells: int = 384, thickness: float = 0.04, periods: float = 2.0):
+    """Thin gyroid sheet |sin x cos y + sin y cos z + sin z cos x| <= thickness over
+    [0, 2*pi*periods]^3, capped by an outside lattice border (closed)."""
+    h = _meshgen().mg_gyroid(cells + 1, 0.0, 2.0 * np.pi * periods, thickness)
+    return _collect(h)
+
+
+def mc_table():
+    """The derived marching-cubes table: (256, 16, 3) edge ids (-1 padded), (12, 2) edge corners."""
+    import ctypes
+
+    tri = np.empty(256 * 48, dtype=np.int8); ec = np.empty(24, dtype=np.int32)
+    _meshgen().mg_table(tri.ctypes.data_as(ctypes.POINTER(ctypes.c_int8)), ec.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+    return tri.reshape(256, 16, 3), ec.reshape(12, 2)
+
+
+def is_oriented(IEN: np.ndarray) -> bool:
+    """Every directed edge appears once and its reverse once (consistently oriented, closed)."""
+    F = np.asarray(IEN, dtype=np.int64)
+    d = np.concatenate([F[:, [0, 1]], F[:, [1, 2]], F[:, [2, 0]]])
+    key = d[:, 0] * (F.max() + 1) + d[:, 1]
+    rkey = d[:, 1] * (F.max() + 1) + d[:, 0]
+    u, cnt = np.unique(key, return_counts=True)
+    return bool(np.all(cnt == 1) and np.array_equal(np.sort(key), np.sort(rkey)))
+
+
+def signed_volume(X: np.ndarray, IEN: np.ndarray) -> float:
+    F = np.asarray(IEN, dtype=np.int64) - 1
+    a, b, c = X[F[:, 0]], X[F[:, 1]], X[F[:, 2]]
+    return float(np.einsum("ij,ij->i", a, np.cross(b, c)).sum() / 6.0)
+
+
 def is_closed(IEN: np.ndarray) -> bool:
     """Every undirected edge is used by exactly two triangles."""
     F = np.asarray(IEN, dtype=np.int64)

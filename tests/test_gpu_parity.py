@@ -216,3 +216,55 @@ def test_errors_are_reported(gpu_ctx):
     with pytest.raises(_native.SdfGpuError):
         ctx.signs([0, 0, 0], 0.1, [3, 3, 3], min_rays=0)
     ctx.close()
+
+
+def test_blobs_small_full(gpu_ctx):
+    """Marching-cubes blob mesh (16 blobs, 96^3 lattice) on a 64-node grid, every node."""
+    from stl2sdf import DataImport, synthetic
+
+    V, F = synthetic.blobs(16, seed=5, cells=96)
+    X, IEN = DataImport.roundtrip_float32(V, F)
+    g = grid_of(X, n_nodes_long_axis=64)
+    d, dr, _, _, fl = run_pair(gpu_ctx, X, IEN, g, mode=0)
+    check_dist(d, dr, X)
+    s, c = gpu_ctx.signs(g["origin"], g["h"], g["N"])
+    ref = oracle.signs(X, IEN, g["origin"], g["h"], g["N"])
+    assert np.array_equal(s, ref["sign"]) and np.array_equal(c, ref["conf"])
+
+
+def test_gyroid_small_full(gpu_ctx):
+    """Capped gyroid sheet (one period, 48^3 lattice): thin walls, grazing axis rays, adaptive
+    vote and winding fallback; every node of a 48-node grid."""
+    from stl2sdf import DataImport, synthetic
+
+    V, F = synthetic.gyroid(48, 0.04, 1.0)
+    X, IEN = DataImport.roundtrip_float32(V, F)
+    g = grid_of(X, n_nodes_long_axis=48)
+    d, dr, _, _, _ = run_pair(gpu_ctx, X, IEN, g, mode=0)
+    check_dist(d, dr, X)
+    d, dr, _, _, _ = run_pair(gpu_ctx, X, IEN, g, mode=1)
+    check_dist(d, dr, X)
+    s, c = gpu_ctx.signs(g["origin"], g["h"], g["N"])
+    st = gpu_ctx.stats()
+    ref = oracle.signs(X, IEN, g["origin"], g["h"], g["N"])
+    assert np.array_equal(s, ref["sign"]) and np.array_equal(c, ref["conf"])
+    assert st["undecided_nodes"] == int(np.count_nonzero(ref["rays"] > 6))
+
+
+def test_blobs_full_size_sample(gpu_ctx):
+    """Workload 3 mesh (64 blobs at 512^3, ~1.4M triangles) on its 256-node grid: every node on the
+    GPU, a seeded sample of 3,000 nodes in the oracle; plus size-independent properties."""
+    from stl2sdf import DataImport, synthetic
+
+    V, F = synthetic.blobs(64, seed=2, cells=512)
+    X, IEN = DataImport.roundtrip_float32(V, F)
+    g = grid_of(X, n_nodes_long_axis=256)
+    gpu_ctx.set_mesh(X, IEN)
+    sdf, dist, sign, conf = gpu_ctx.sdf(g["origin"], g["h"], g["N"], want_parts=True)
+    assert np.all((dist >= 0) & (dist <= g["h"]))
+    assert np.all(np.abs(sign) == 1.0) and np.array_equal(sdf, dist * sign)
+    nodes = sample_nodes(g["ngp"], 3000, seed=11)
+    dr, _, _ = oracle.distances(X, IEN, g["origin"], g["h"], g["N"], mode=0, nodes=nodes)
+    check_dist(dist[nodes], dr, X)
+    ref = oracle.signs(X, IEN, g["origin"], g["h"], g["N"], nodes=nodes)
+    assert np.array_equal(sign[nodes], ref["sign"]) and np.array_equal(conf[nodes], ref["conf"])
