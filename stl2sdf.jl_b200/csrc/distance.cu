@@ -29,6 +29,7 @@
 #include <cub/cub.cuh>
 
 #include "common.cuh"
+#include "fold32.cuh"
 
 namespace sdfgpu {
 
@@ -140,22 +141,26 @@ struct FoldArgs {
   int64_t* counters;
 };
 
-// Per-warp shared staging of 32 list entries: FP32 vertices and centroid (64 B each) and, per
-// (entry, lane), the FP32 distance that passed the filter.
+// Per-warp shared staging of 32 list entries in the tile's local frame (origin = the tile's first
+// node): the candidate for the FP32 step, its centroid and box, and per (entry, lane) the FP32
+// point-triangle distance that survived phase A.
 struct __align__(16) WarpStage {
-  float4 v[32][3];
-  float4 c[32];
-  float4 lo[32], hi[32];  // FP32 box of the entry
-  int32_t id[32];
-  float D[32][32];  // [entry][lane]
+  Cand32 c[32];
+  float4 cc[32];          // centroid - origin; .w = |centroid - origin|
+  float4 lo[32], hi[32];  // box of the triangle in the local frame
+  float D2[32][32];       // [entry][lane]: squared FP32 point-triangle distance
 };
 
 // One CTA per tile, one lane per node.  The tile's ascending triangle list is consumed 32 entries
-// at a time.  Phase A (convergent FP32): every lane tests each staged entry against its own node
-// (centroid ball, then point-triangle distance D against the running minimum m) and sets a bit
-// per surviving entry.  Phase B: lanes drain their bits lowest-first, i.e. in ascending triangle
-// index, so all lanes execute the FP64 reference step together on different triangles instead of
-// one lane at a time; an entry whose D now exceeds the (smaller) running minimum is dropped.
+// at a time.
+//   Phase A (FP32, all lanes in step): centroid-ball test (FP64 only inside its error band), box
+//   test and point-triangle distance D against the running minimum m: an entry farther than m
+//   cannot change the fold, because every value the reference step assigns is at least the true
+//   point-triangle distance.
+//   Phase B: lanes drain their surviving entries lowest-first (ascending triangle index) through
+//   the FP32 replay of the reference step (fold32.cuh).  Only a decision inside its error band
+//   runs the FP64 reference step (exact64.cuh); the FP64 value of the final winner is recomputed
+//   once, so the output has the reference arithmetic's bits.
 __global__ void __launch_bounds__(256) k_tile_fold(FoldArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpStage& S = reinterpret_cast<WarpStage*>(smem_raw)[threadIdx.x >> 5];
@@ -168,39 +173,52 @@ __global__ void __launch_bounds__(256) k_tile_fold(FoldArgs A) {
   const bool valid = i <= g.N[0] && j <= g.N[1] && k <= g.N[2];
   const int64_t lin = i + g.n[0] * (j + g.n[1] * k);
   const d3 p = node_coord(g.o, g.h, i, j, k);
-  const float3 p32 = local32(g, p);
+  const d3 t0 = node_coord(g.o, g.h, tx * g.t[0], ty * g.t[1], tz * g.t[2]);
+  const float3 pl = make_float3((float)(p.x - t0.x), (float)(p.y - t0.y), (float)(p.z - t0.z));
+  const float plen = len3(pl);
+  const float sr = (float)(2.5 * g.h);
   const int32_t start = A.tile_off[tile], end = start + A.tile_cnt[tile];
   const bool ref = A.mode == SDFGPU_MODE_REF_RULE;
-  double m = kBig;
+  // running minimum: FP32 estimate m32 (error em), exact m64 when m64_ok, else the winner to
+  // recompute it from
+  double m64 = kBig;
   d3 proj = {0.0, 0.0, 0.0};
-  bool have = false, any = false;
+  bool m64_ok = true, any = false;
+  float m32 = (float)kBig, em = 0.f;
+  int win_tri = -1, win_feat = 0, win_gid = -1;
   int64_t fp64 = 0;
   for (int32_t base = start; base < end; base += 32) {
     const int nE = min(32, end - base);
     if ((int)lane < nE) {
       const int32_t tri = __ldg(&A.vals[base + lane]);
-      S.id[lane] = tri;
-      S.v[lane][0] = __ldg(&A.v32[3 * tri]);
-      S.v[lane][1] = __ldg(&A.v32[3 * tri + 1]);
-      S.v[lane][2] = __ldg(&A.v32[3 * tri + 2]);
-      S.c[lane] = __ldg(&A.c32[tri]);
-      const float4 a = S.v[lane][0], b = S.v[lane][1], c = S.v[lane][2];
-      S.lo[lane] = make_float4(fminf(a.x, fminf(b.x, c.x)), fminf(a.y, fminf(b.y, c.y)), fminf(a.z, fminf(b.z, c.z)), 0.f);
-      S.hi[lane] = make_float4(fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y)), fmaxf(a.z, fmaxf(b.z, c.z)), 0.f);
+      const TriRec64& r = A.rec[tri];
+      const d3 v0 = rec_v(r, 0), v1 = rec_v(r, 1), v2 = rec_v(r, 2);
+      const float3 a = make_float3((float)(v0.x - t0.x), (float)(v0.y - t0.y), (float)(v0.z - t0.z));
+      const float3 e1 = make_float3((float)(v1.x - v0.x), (float)(v1.y - v0.y), (float)(v1.z - v0.z));
+      const float3 e2 = make_float3((float)(v2.x - v0.x), (float)(v2.y - v0.y), (float)(v2.z - v0.z));
+      const bool ok = __ldg(&A.c32[tri]).w != 0.f;
+      make_cand(a, e1, e2, ok, __float_as_int(__ldg(&A.v32[3 * tri]).w), __float_as_int(__ldg(&A.v32[3 * tri + 1]).w),
+                __float_as_int(__ldg(&A.v32[3 * tri + 2]).w), tri, S.c[lane]);
+      const double4 cd = A.cent[tri];
+      const float3 cc = make_float3((float)(cd.x - t0.x), (float)(cd.y - t0.y), (float)(cd.z - t0.z));
+      S.cc[lane] = make_float4(cc.x, cc.y, cc.z, len3(cc));
+      const float3 b = a + e1, q = a + e2;
+      S.lo[lane] = make_float4(fminf(a.x, fminf(b.x, q.x)), fminf(a.y, fminf(b.y, q.y)), fminf(a.z, fminf(b.z, q.z)), 0.f);
+      S.hi[lane] = make_float4(fmaxf(a.x, fmaxf(b.x, q.x)), fmaxf(a.y, fmaxf(b.y, q.y)), fmaxf(a.z, fmaxf(b.z, q.z)), 0.f);
     }
     __syncwarp();
     uint32_t bits = 0;
     if (valid) {
-      const float lim = have ? (float)m + A.eD_abs + A.eD_rel * (float)m : 1.0e18f;
       for (int q = 0; q < nE; ++q) {
         if (ref) {
-          const float4 c = S.c[q];
-          const float dx = c.x - p32.x, dy = c.y - p32.y, dz = c.z - p32.z;
+          const float4 cc = S.cc[q];
+          const float dx = cc.x - pl.x, dy = cc.y - pl.y, dz = cc.z - pl.z;
           const float s32 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          if (s32 > A.r2_out) continue;
-          if (s32 >= A.r2_in) {  // inside the FP32 error band: the reference's FP64 test decides
-            const double4 cc = A.cent[S.id[q]];
-            const double ex = ds(cc.x, p.x), ey = ds(cc.y, p.y), ez = ds(cc.z, p.z);
+          const float ec = kU * 16.f * (plen + cc.w);
+          if (s32 > (sr + ec) * (sr + ec)) continue;
+          if (s32 >= (sr - ec) * (sr - ec)) {  // inside the FP32 error band: the reference's test decides
+            const double4 cd = A.cent[S.c[q].gid.w];
+            const double ex = ds(cd.x, p.x), ey = ds(cd.y, p.y), ez = ds(cd.z, p.z);
             double s = dm(ex, ex);
             s = da(s, dm(ey, ey));
             s = da(s, dm(ez, ez));
@@ -208,13 +226,14 @@ __global__ void __launch_bounds__(256) k_tile_fold(FoldArgs A) {
           }
         }
         any = true;
-        // box reject (the reference's point_in_box_range against the running minimum, with the
-        // FP32 margin): a triangle whose box is farther than m cannot change the fold
-        if (box_d2(p32, f3(S.lo[q]), f3(S.hi[q])) > lim * lim) continue;
-        const float D = sqrtf(pt_tri_d2(p32, f3(S.v[q][0]), f3(S.v[q][1]), f3(S.v[q][2])));
-        if (D <= lim) {
+        const Cand32& c = S.c[q];
+        const float lim = m32 + em + cand_err(c, plen);
+        const float lim2 = lim * lim;
+        if (box_d2(pl, f3(S.lo[q]), f3(S.hi[q])) > lim2) continue;
+        const float D2 = cand_d2(pl, c);
+        if (D2 <= lim2) {
           bits |= 1u << q;
-          S.D[q][lane] = D;
+          S.D2[q][lane] = D2;
         }
       }
     }
@@ -222,10 +241,30 @@ __global__ void __launch_bounds__(256) k_tile_fold(FoldArgs A) {
       if (bits) {
         const int q = __ffs(bits) - 1;
         bits &= bits - 1;
-        if (!have || (double)S.D[q][lane] <= m + (double)(A.eD_abs + A.eD_rel * (float)m)) {
-          tri_step64(A.rec[S.id[q]], p, m, proj, ref);
-          have = true;
-          ++fp64;
+        const Cand32& c = S.c[q];
+        const float lim = m32 + em + cand_err(c, plen);
+        if (S.D2[q][lane] <= lim * lim) {
+          float val, err;
+          int feat;
+          const int act = step32(pl, plen, c, m32, em, ref, win_gid, val, feat, err);
+          if (act == S_ASSIGN) {
+            m32 = val;
+            em = err;
+            win_tri = c.gid.w;
+            win_feat = feat;
+            win_gid = feat >= F_VERT0 ? (feat == F_VERT0 ? c.gid.x : (feat == F_VERT1 ? c.gid.y : c.gid.z)) : -1;
+            m64_ok = false;
+          } else if (act == S_AMBIG) {
+            if (!m64_ok) {
+              feature64(A.rec[win_tri], p, win_feat, m64, proj);
+              m64_ok = true;
+            }
+            tri_step64(A.rec[c.gid.w], p, m64, proj, ref);
+            m32 = (float)m64;
+            em = kU * 2.f * m32;
+            win_gid = -1;
+            ++fp64;
+          }
         }
       }
     }
@@ -233,7 +272,13 @@ __global__ void __launch_bounds__(256) k_tile_fold(FoldArgs A) {
   }
   int cand = 0;
   if (valid) {
-    double d = m;
+    const bool clamped = m32 - em > (float)g.h * (1.0f + 4.0f * kU);
+    if (!m64_ok && (!clamped || A.xp)) {
+      feature64(A.rec[win_tri], p, win_feat, m64, proj);
+      m64_ok = true;
+      ++fp64;
+    }
+    double d = m64_ok ? m64 : g.h;
     if (fabs(d) > fabs(g.h)) d = g.h;  // clamp (dfOnTriangularMesh.jl:202-206)
     A.dist[lin] = d;
     if (A.xp) {

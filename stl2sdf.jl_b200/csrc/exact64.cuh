@@ -246,6 +246,28 @@ __device__ inline void tri_step64(const TriRec64& r, const d3& p, double& m, d3&
   }
 }
 
+// Features a reference step can assign to the running minimum.
+enum Feature : int { F_FACE = 0, F_EDGE0 = 1, F_EDGE1 = 2, F_EDGE2 = 3, F_VERT0 = 4, F_VERT1 = 5, F_VERT2 = 6 };
+
+// The value (and closest point) tri_step64 assigns when `feat` wins: the same expressions, so the
+// result has the same bits.
+__device__ __forceinline__ void feature64(const TriRec64& r, const d3& p, int feat, double& d, d3& xp) {
+  if (feat == F_FACE) {
+    double lam[3];
+    bary_solve(r, p, lam);
+    xp = v_add(v_add(v_scale(rec_v(r, 0), lam[0]), v_scale(rec_v(r, 1), lam[1])), v_scale(rec_v(r, 2), lam[2]));
+  } else if (feat <= F_EDGE2) {
+    const int j = feat - F_EDGE0;
+    const d3 vj = rec_v(r, j);
+    const d3 u = {r.u[3 * j], r.u[3 * j + 1], r.u[3 * j + 2]};
+    const double P = v_dot(v_sub(p, vj), u);
+    xp = v_add(vj, v_scale(u, P));
+  } else {
+    xp = rec_v(r, feat - F_VERT0);
+  }
+  d = v_norm(v_sub(p, xp));
+}
+
 // Möller–Trumbore with the reference's decisions (RaycastingSignDetection.jl:64-106).
 __device__ __forceinline__ bool mt64(const d3& o, const d3& d, const d3& v1, const d3& v2, const d3& v3,
                                      double eps, double& tout) {

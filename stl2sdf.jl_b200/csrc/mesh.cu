@@ -87,20 +87,40 @@ __global__ void k_prep(const double* __restrict__ X, int64_t nnp, const int64_t*
 
 // Mesh-local FP32 copies: vertices, centroid, outward-rounded box; and rho = max vertex
 // distance from the centroid (decides whether the centroid rule can miss a triangle within h).
-__global__ void k_local32(const TriRec64* __restrict__ rec, const double4* __restrict__ cent, int64_t nel, double cx,
-                          double cy, double cz, float4* __restrict__ v32, float4* __restrict__ c32,
-                          float4* __restrict__ box32, unsigned long long* rho_ord) {
+// v32[3*el+k].w carries the global (0-based) index of vertex k; c32[el].w is 1 when the triangle
+// is well conditioned for FP32 decisions (no edge shorter than 1e-5 E, sine of the smallest
+// angle above ~1e-3, distinct vertices) and 0 when every decision on it must be made in FP64.
+__global__ void k_local32(const TriRec64* __restrict__ rec, const double4* __restrict__ cent,
+                          const int64_t* __restrict__ IEN, int64_t nel, double cx, double cy, double cz, double E,
+                          float4* __restrict__ v32, float4* __restrict__ c32, float4* __restrict__ box32,
+                          unsigned long long* rho_ord) {
   double rho = 0.0;
   for (int64_t el = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; el < nel; el += (int64_t)gridDim.x * blockDim.x) {
     const TriRec64& r = rec[el];
     const double4 c = cent[el];
+    int32_t gid[3];
     for (int k = 0; k < 3; ++k) {
+      gid[k] = (int32_t)(IEN[3 * el + k] - 1);
       const double x = r.v[3 * k], y = r.v[3 * k + 1], z = r.v[3 * k + 2];
-      v32[3 * el + k] = make_float4((float)(x - cx), (float)(y - cy), (float)(z - cz), 0.f);
+      v32[3 * el + k] = make_float4((float)(x - cx), (float)(y - cy), (float)(z - cz), __int_as_float(gid[k]));
       const double dx = x - c.x, dy = y - c.y, dz = z - c.z;
       rho = fmax(rho, sqrt(dx * dx + dy * dy + dz * dz));
     }
-    c32[el] = make_float4((float)(c.x - cx), (float)(c.y - cy), (float)(c.z - cz), 0.f);
+    double L[3], lmin = 1e300, lmax = 0.0;
+    for (int j = 0; j < 3; ++j) {
+      const int a = j, b = (j + 1) % 3;
+      const double ex = r.v[3 * b] - r.v[3 * a], ey = r.v[3 * b + 1] - r.v[3 * a + 1], ez = r.v[3 * b + 2] - r.v[3 * a + 2];
+      L[j] = sqrt(ex * ex + ey * ey + ez * ez);
+      lmin = fmin(lmin, L[j]);
+      lmax = fmax(lmax, L[j]);
+    }
+    const double ax = r.v[3] - r.v[0], ay = r.v[4] - r.v[1], az = r.v[5] - r.v[2];
+    const double bx = r.v[6] - r.v[0], by = r.v[7] - r.v[1], bz = r.v[8] - r.v[2];
+    const double nx = ay * bz - az * by, ny = az * bx - ax * bz, nz = ax * by - ay * bx;
+    const double nn = sqrt(nx * nx + ny * ny + nz * nz);
+    const bool ok = lmin > 1e-5 * E && nn > 1e-3 * lmax * lmax && gid[0] != gid[1] && gid[1] != gid[2] &&
+                    gid[0] != gid[2];
+    c32[el] = make_float4((float)(c.x - cx), (float)(c.y - cy), (float)(c.z - cz), ok ? 1.f : 0.f);
     box32[2 * el] = make_float4(__double2float_rd(r.bmin[0] - cx), __double2float_rd(r.bmin[1] - cy),
                                 __double2float_rd(r.bmin[2] - cz), 0.f);
     box32[2 * el + 1] = make_float4(__double2float_ru(r.bmax[0] - cx), __double2float_ru(r.bmax[1] - cy),
@@ -283,8 +303,8 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
 
   unsigned long long rho0 = 0ULL;  // below the encoding of every non-negative double
   SDF_CUDA(ctx, cudaMemcpyAsync(bb + 7, &rho0, sizeof(rho0), cudaMemcpyHostToDevice, st));
-  k_local32<<<grid_for(nel, 128), 128, 0, st>>>(rec, cent, nel, M.center[0], M.center[1], M.center[2], v32, c32,
-                                                 box32, bb + 7);
+  k_local32<<<grid_for(nel, 128), 128, 0, st>>>(rec, cent, dIEN, nel, M.center[0], M.center[1], M.center[2], M.E, v32,
+                                                 c32, box32, bb + 7);
   SDF_KERNEL(ctx);
 
   // LBVH
