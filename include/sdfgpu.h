@@ -153,6 +153,23 @@ int sdfgpu_sdf_device(sdfgpu_ctx* ctx, const double origin[3], double h, const i
                       double confidence_threshold, int32_t use_winding_fallback, double* d_sdf,
                       double* d_dist, double* d_sign, double* d_conf);
 
+/* Allocation-free distances.  No counterpart in the reference: it exists for callers that must
+ * not allocate GPU memory -- code running inside a host callback or an allocator hook, processes
+ * whose device memory belongs to another framework's pool, or real-time loops that cannot take the
+ * allocator's locks.  Every other entry point allocates its scratch on first use; this one keeps
+ * its only scratch (the per-triangle records) in a fixed device array of about 5.8 MB that every
+ * GPU loading the library holds until the process exits, and calls no allocator.
+ *   d_X (3 x nnp), d_IEN (3 x nel, 1-based) and d_dist_out (ngp doubles) are device memory of the
+ *   current device; mode is SDFGPU_MODE_EXACT or SDFGPU_MODE_UNBOUNDED; stream may be NULL.
+ *   At most 16384 triangles (SDFGPU_ERR_CAPACITY beyond).  The result equals sdfgpu_distances in
+ *   the same mode.  Returns after the stream has finished; errors go to sdfgpu_last_error(NULL).
+ *   Every call reuses the same array: calls that overlap on the GPU race, so serialise them.
+ *   The first call on a device looks up the array's address with that device current; make it
+ *   before any stream capture. */
+int sdfgpu_distances_noalloc(const double* d_X, int64_t nnp, const int64_t* d_IEN, int64_t nel,
+                             const double origin[3], double h, const int64_t N[3], int32_t mode,
+                             double* d_dist_out, void* stream);
+
 /* The cudaStream_t every kernel of the context runs on. */
 int sdfgpu_get_stream(sdfgpu_ctx* ctx, void** stream);
 int sdfgpu_get_stats(const sdfgpu_ctx* ctx, sdfgpu_stats* out);

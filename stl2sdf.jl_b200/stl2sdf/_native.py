@@ -75,6 +75,8 @@ SIGNATURES = {
     "sdfgpu_sdf_device": ([ctypes.c_void_p, _dp, ctypes.c_double, _i64p, ctypes.c_int32, ctypes.c_int32,
                            ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                            ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "sdfgpu_distances_noalloc": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, _dp,
+                                  ctypes.c_double, _i64p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "sdfgpu_get_stream": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "sdfgpu_get_stats": ([ctypes.c_void_p, ctypes.POINTER(Stats)], ctypes.c_int),
 }
