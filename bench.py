@@ -135,6 +135,39 @@ def cpu_baseline(X, IEN, g, budget_s=12.0, seed=42):
             "sample": f"{nodes.shape[0]} seeded (seed {seed}) uniform grid nodes of the workload, distance+sign, {dt:.1f} s"}
 
 
+def distance_variants(ctx, X, IEN, g, reps=3):
+    """Distance-stage throughput (device time of sdfgpu_distances, mesh resident) of the modes the
+    metric compares: the reference rule (clamped), the true minimum clamped to h, the plain unbounded
+    search and the learned-radius unbounded search (bit-identical to plain), plus the network's
+    training time and certified fraction."""
+    import time as _t
+
+    ctx.set_mesh(X, IEN)
+    out = {}
+
+    def run(mode, learned=False):
+        ms = []
+        for _ in range(reps + 1):
+            ctx.distances(g["origin"], g["h"], g["N"], mode, learned=learned)
+            ms.append(ctx.stats()["ms_distance"])
+        ms = sorted(ms[1:])[len(ms[1:]) // 2]
+        return {"nodes_per_s": g["ngp"] / (ms / 1e3), "ms": ms}
+
+    out["ref_rule"] = run(0)
+    out["exact_h_bounded"] = run(1)
+    out["plain_unbounded"] = run(2)
+    t0 = _t.perf_counter()
+    loss = ctx.train_radius(coarse_n=64, steps=1500, batch=8192)
+    train_s = _t.perf_counter() - t0
+    out["learned_unbounded"] = run(2, learned=True)
+    st = ctx.stats()
+    out["learned_unbounded"].update({"certified_fraction": st["certified_nodes"] / g["ngp"],
+                                     "fallback_nodes": st["unbounded_fallbacks"], "train_s": train_s,
+                                     "train_loss": loss, "train_grid": "64 nodes on the long axis, 1500 Adam steps"})
+    out["learned_vs_plain_unbounded"] = out["plain_unbounded"]["ms"] / out["learned_unbounded"]["ms"]
+    return out
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference algorithm (the oracle restatement) on the host cores."""
     if rank != 0:
@@ -179,6 +212,7 @@ def main():
     ap.add_argument("--impl", default="sdfgpu", choices=["sdfgpu", "reference"])
     ap.add_argument("--workload", default="torus128")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=1 << 14)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -330,6 +364,8 @@ def main():
         "clocks": clk.summary(),
         "wall_s": wall,
     }
+    if not args.no_variants:
+        line["distance_variants"] = distance_variants(ctx, X, IEN, g)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(X, IEN, g)
     if dist_on:

@@ -100,6 +100,8 @@ typedef struct sdfgpu_stats {
   double ms_rows;                 /* axis-row hit lists (count, fill, sort) */
   double ms_parity;               /* the three axis-parity kernels */
   double ms_vote;                 /* vote + adaptive rays + winding */
+  int64_t certified_nodes;        /* learned radius: nodes whose bounded search certified the result */
+  double radius_loss;             /* final training loss of the radius network */
 } sdfgpu_stats;
 
 /* Context lifetime.  opts may be NULL (device 0, default tiles). */
@@ -169,6 +171,31 @@ int sdfgpu_sdf_device(sdfgpu_ctx* ctx, const double origin[3], double h, const i
 int sdfgpu_distances_noalloc(const double* d_X, int64_t nnp, const int64_t* d_IEN, int64_t nel,
                              const double origin[3], double h, const int64_t N[3], int32_t mode,
                              double* d_dist_out, void* stream);
+
+/* Learned search radius for SDFGPU_MODE_UNBOUNDED (the north-star extension of the reference's
+ * distance search; no reference counterpart).  A 3 x 64 Fourier-feature MLP (FP16 weights, FP32
+ * accumulate) is trained on the GPU on the exact unbounded distances of a coarse grid of the current
+ * mesh (coarse_n nodes on its longest axis, Grid(Xmin, Xmax, coarse_n - 7, 3)).  sdfgpu_distances
+ * with use_learned_radius = 1 then bounds each node's search by the predicted radius; a hit inside
+ * it is certified exact, other nodes fall back to the unbounded search (stats: certified_nodes,
+ * unbounded_fallbacks).  Results are bit-identical to the plain unbounded mode. */
+int sdfgpu_train_radius(sdfgpu_ctx* ctx, int32_t coarse_n, int32_t steps, int32_t batch, float lr, uint64_t seed,
+                        float* final_loss);
+/* Number of FP32 parameters of the radius network (layout: W1 64x32, b1, W2 64x64, b2, W3 64x64,
+ * b3, w4 64, b4). */
+int sdfgpu_radius_param_count(void);
+/* Read / replace the network: params (param_count floats, FP32 masters) and the normalisation
+ * norm = {cx, cy, cz, s} of x = (p - c) / s. */
+int sdfgpu_radius_params(sdfgpu_ctx* ctx, float* params, double norm[4]);
+int sdfgpu_set_radius_params(sdfgpu_ctx* ctx, const float* params, const double norm[4]);
+/* Network output dhat (normalised distance) at B normalised points xn (B x 3, host), evaluated by
+ * the tensor-core inference kernel. */
+int sdfgpu_radius_eval(sdfgpu_ctx* ctx, const float* xn, int64_t B, float* dhat);
+/* The training forward and backward of the network at host params over B samples (host): dhat,
+ * the loss and the FP32 parameter gradient (any output may be NULL).  Used to check the GPU
+ * gradients against a CPU implementation. */
+int sdfgpu_mlp_train_eval(sdfgpu_ctx* ctx, const float* params, const float* xn, const float* target, int64_t B,
+                          float* dhat, float* loss, float* grad);
 
 /* The cudaStream_t every kernel of the context runs on. */
 int sdfgpu_get_stream(sdfgpu_ctx* ctx, void** stream);

@@ -199,6 +199,8 @@ int finish_counters(sdfgpu_ctx* ctx, const GridP& g) {
   s.winding_ambiguous = c[C_WIND_AMBIG];
   s.unbounded_fallbacks = c[C_UNB_FALLBACK];
   s.rho_max = ctx->mesh.rho_max;
+  s.certified_nodes = c[C_CERTIFIED];
+  s.radius_loss = ctx->radius.loss;
   if (c[C_ERR_STACK]) return fail(ctx, SDFGPU_ERR_CAPACITY, "BVH traversal stack overflow");
   if (c[C_ERR_CAPACITY])
     return fail(ctx, SDFGPU_ERR_CAPACITY, "a per-node hit or candidate buffer overflowed (" + std::to_string(c[C_ERR_CAPACITY]) + " nodes)");
@@ -217,6 +219,8 @@ int check_mode(sdfgpu_ctx* ctx, int mode, int learned) {
     return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "unknown distance mode");
   if (learned && mode != SDFGPU_MODE_UNBOUNDED)
     return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "use_learned_radius needs SDFGPU_MODE_UNBOUNDED");
+  if (learned && !ctx->radius.trained)
+    return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "use_learned_radius: no radius network (sdfgpu_train_radius)");
   return 0;
 }
 
@@ -444,6 +448,51 @@ int sdfgpu_sdf(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t 
   if (conf_out) SDF_CUDA(ctx, cudaMemcpyAsync(conf_out, d_conf, bytes, cudaMemcpyDeviceToHost, st));
   SDF_CUDA(ctx, cudaStreamSynchronize(st));
   return SDFGPU_OK;
+}
+
+int sdfgpu_train_radius(sdfgpu_ctx* ctx, int32_t coarse_n, int32_t steps, int32_t batch, float lr, uint64_t seed,
+                        float* final_loss) {
+  SDF_TRY(begin_call(ctx));
+  SDF_TRY(need_mesh(ctx));
+  if (coarse_n < 9 || coarse_n > 1024 || steps < 0 || batch < 32 || !(lr > 0.f))
+    return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "train_radius: need 9 <= coarse_n <= 1024, steps >= 0, batch >= 32, lr > 0");
+  SDF_TRY(reset_counters(ctx));
+  return train_radius(ctx, coarse_n, steps, batch, lr, seed, final_loss);
+}
+
+int sdfgpu_radius_param_count(void) { return kParams; }
+
+int sdfgpu_radius_params(sdfgpu_ctx* ctx, float* params, double norm[4]) {
+  SDF_TRY(begin_call(ctx));
+  if (!params || !norm) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "NULL argument");
+  return get_radius_params(ctx, params, norm);
+}
+
+int sdfgpu_set_radius_params(sdfgpu_ctx* ctx, const float* params, const double norm[4]) {
+  SDF_TRY(begin_call(ctx));
+  if (!params || !norm || !(norm[3] > 0.0)) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "bad params or norm");
+  return set_radius_params(ctx, params, norm);
+}
+
+int sdfgpu_radius_eval(sdfgpu_ctx* ctx, const float* xn, int64_t B, float* dhat) {
+  SDF_TRY(begin_call(ctx));
+  if (!xn || !dhat || B < 1) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "bad arguments");
+  float *dx, *dy;
+  SDF_TRY(scratch_t(ctx, "reval_x", (size_t)B * 3, &dx));
+  SDF_TRY(scratch_t(ctx, "reval_y", (size_t)B, &dy));
+  SDF_CUDA(ctx, cudaMemcpyAsync(dx, xn, sizeof(float) * 3 * B, cudaMemcpyHostToDevice, ctx->stream));
+  SDF_TRY(run_radius(ctx, nullptr, dx, B, -1.f, 0.f, dy));
+  SDF_CUDA(ctx, cudaMemcpyAsync(dhat, dy, sizeof(float) * B, cudaMemcpyDeviceToHost, ctx->stream));
+  SDF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return SDFGPU_OK;
+}
+
+int sdfgpu_mlp_train_eval(sdfgpu_ctx* ctx, const float* params, const float* xn, const float* target, int64_t B,
+                          float* dhat, float* loss, float* grad) {
+  SDF_TRY(begin_call(ctx));
+  if (!params || !xn || B < 1) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "bad arguments");
+  if ((loss || grad) && !target) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "loss and gradient need targets");
+  return mlp_eval_host(ctx, params, xn, target, B, dhat, loss, grad);
 }
 
 int sdfgpu_get_stream(sdfgpu_ctx* ctx, void** stream) {

@@ -9,6 +9,7 @@
 
 #include "exact64.cuh"
 #include "geom32.cuh"
+#include "radius.cuh"
 #include "sdfgpu.h"
 
 namespace sdfgpu {
@@ -42,6 +43,7 @@ enum Counter : int {
   C_ERR_INDEX,      // mesh index out of range
   C_LIST_UNDECIDED, // length of the undecided-node list
   C_LIST_WINDING,   // length of the winding list
+  C_CERTIFIED,      // learned radius: nodes certified by the bounded search
   C_NUM = 32
 };
 
@@ -87,6 +89,7 @@ struct sdfgpu_ctx {
   int64_t* d_counters = nullptr;
   int64_t h_counters[sdfgpu::C_NUM] = {};
   sdfgpu_stats stats = {};
+  sdfgpu::RadiusNorm radius;  // learned search radius (radius.cu)
   int64_t launches = 0;  // kernels of this library launched since the last reset
   cudaEvent_t tev[8] = {};  // stage timestamps, see sdfgpu::Stage
 };
@@ -174,6 +177,12 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
 int run_signs(sdfgpu_ctx* ctx, const GridP& g, int min_rays, int max_rays, double conf_thresh, int use_winding,
               const double* d_dist, double* d_sign, double* d_conf, double* d_sdf);
 int cub_scan_i32(sdfgpu_ctx* ctx, const int32_t* in, int32_t* out, int64_t n);
+int train_radius(sdfgpu_ctx* ctx, int coarse_n, int steps, int batch, float lr, uint64_t seed, float* final_loss);
+int set_radius_params(sdfgpu_ctx* ctx, const float* params, const double norm[4]);
+int get_radius_params(sdfgpu_ctx* ctx, float* params, double norm[4]);
+int run_radius(sdfgpu_ctx* ctx, const GridP* g, const float* d_pts, int64_t count, float alpha, float beta, float* d_out);
+int mlp_eval_host(sdfgpu_ctx* ctx, const float* params, const float* xn, const float* target, int64_t B, float* yhat,
+                  float* loss, float* grad);
 int cub_scan_i64(sdfgpu_ctx* ctx, const int64_t* in, int64_t* out, int64_t n);
 
 }  // namespace sdfgpu

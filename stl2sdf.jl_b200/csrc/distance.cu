@@ -450,16 +450,64 @@ struct UnbArgs {
   float pad;
   float eD_abs, eD_rel;
   int64_t max_visits;
+  const float* radius;  // learned radius per node (nullable)
   double* dist;
   double* xp;
   int64_t* counters;
 };
 
-// True nearest triangle (no clamp): depth-first LBVH search, nearer child first, FP32 bounds,
-// FP64 reference arithmetic for the candidates inside the FP32 error band.
+// Depth-first LBVH nearest search from node p, nearer child first.  Boxes farther than the bound
+// (the running minimum plus the FP32 margin, or `r0` before the first hit) are pruned; candidates
+// inside the FP32 error band of the running minimum get the FP64 reference step (true minimum).
+// Returns false when a visit or stack bound is exceeded.
+__device__ bool nearest(const UnbArgs& A, const d3& p, const float3& p32, float r0, double& m, d3& proj, bool& have,
+                        int64_t& fp64) {
+  int stack[kStack];
+  int sp = 0;
+  stack[sp++] = 0;
+  int64_t visits = 0;
+  while (sp > 0) {
+    if (++visits > A.max_visits) return false;
+    const BNode nd = A.nodes[stack[--sp]];
+    const float bound = have ? (float)m + A.eD_abs + A.eD_rel * (float)m + A.pad : r0 + A.pad;
+    float3 lo0, hi0, lo1, hi1;
+    child_box(nd, 0, lo0, hi0);
+    child_box(nd, 1, lo1, hi1);
+    float d0 = lo0.x > hi0.x ? INFINITY : box_d2(p32, lo0, hi0);
+    float d1 = lo1.x > hi1.x ? INFINITY : box_d2(p32, lo1, hi1);
+    const float b2 = bound * bound;
+    int c0 = nd.d.x, c1 = nd.d.y;
+    if (d1 < d0) {  // visit the nearer child first: push it last
+      float t = d0; d0 = d1; d1 = t;
+      int c = c0; c0 = c1; c1 = c;
+    }
+    const int cs[2] = {c1, c0};
+    const float ds2[2] = {d1, d0};
+    for (int q = 0; q < 2; ++q) {
+      if (isinf(ds2[q]) || !(ds2[q] <= b2)) continue;
+      if (cs[q] & kLeafBit) {
+        const int prim = A.leaf_prim[cs[q] & 0x7fffffff];
+        const float D = sqrtf(pt_tri_d2(p32, f3(A.v32[3 * prim]), f3(A.v32[3 * prim + 1]), f3(A.v32[3 * prim + 2])));
+        if (have && (double)D > m + (double)(A.eD_abs + A.eD_rel * (float)m)) continue;
+        if (!have && D > r0 + A.eD_abs + A.eD_rel * r0) continue;
+        tri_step64(A.rec[prim], p, m, proj, false);
+        have = true;
+        ++fp64;
+      } else {
+        if (sp >= kStack) return false;
+        stack[sp++] = cs[q];
+      }
+    }
+  }
+  return true;
+}
+
+// True nearest triangle of every node (no clamp).  With a learned radius r the first search is
+// bounded by r; a hit with d <= r is certified exact (every nearer triangle lies within r and was
+// visited), otherwise the node searches again without the bound.
 __global__ void __launch_bounds__(128) k_unbounded(UnbArgs A) {
   const GridP& g = A.g;
-  int64_t fp64 = 0;
+  int64_t fp64 = 0, cert = 0, fallback = 0;
   for (int64_t lin = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; lin < g.ngp; lin += (int64_t)gridDim.x * blockDim.x) {
     int64_t i, j, k;
     node_ijk(g, lin, i, j, k);
@@ -467,48 +515,21 @@ __global__ void __launch_bounds__(128) k_unbounded(UnbArgs A) {
     const float3 p32 = local32(g, p);
     double m = kBig;
     d3 proj = {0.0, 0.0, 0.0};
-    bool have = false, overflow = false;
-    int stack[kStack];
-    int sp = 0;
-    stack[sp++] = 0;
-    int64_t visits = 0;
-    while (sp > 0) {
-      if (++visits > A.max_visits) { overflow = true; break; }
-      const BNode nd = A.nodes[stack[--sp]];
-      const float bound = have ? (float)m + A.eD_abs + A.eD_rel * (float)m + A.pad : INFINITY;
-      float3 lo0, hi0, lo1, hi1;
-      child_box(nd, 0, lo0, hi0);
-      child_box(nd, 1, lo1, hi1);
-      float d0 = lo0.x > hi0.x ? INFINITY : box_d2(p32, lo0, hi0);
-      float d1 = lo1.x > hi1.x ? INFINITY : box_d2(p32, lo1, hi1);
-      const float b2 = bound * bound;
-      int c0 = nd.d.x, c1 = nd.d.y;
-      if (d1 < d0) {  // visit the nearer child first: push it last
-        float t = d0; d0 = d1; d1 = t;
-        int c = c0; c0 = c1; c1 = c;
+    bool have = false;
+    bool ok;
+    if (A.radius) {
+      const float r = A.radius[lin];
+      ok = nearest(A, p, p32, r, m, proj, have, fp64);
+      if (ok && have && m <= (double)r) {
+        ++cert;
+      } else if (ok) {
+        ++fallback;
+        ok = nearest(A, p, p32, INFINITY, m, proj, have, fp64);
       }
-      const int cs[2] = {c1, c0};
-      const float ds2[2] = {d1, d0};
-      for (int q = 0; q < 2; ++q) {
-        if (!(ds2[q] <= b2) && have) continue;
-        if (isinf(ds2[q])) continue;
-        if (cs[q] & kLeafBit) {
-          const int prim = A.leaf_prim[cs[q] & 0x7fffffff];
-          if (have) {
-            const float D = sqrtf(pt_tri_d2(p32, f3(A.v32[3 * prim]), f3(A.v32[3 * prim + 1]), f3(A.v32[3 * prim + 2])));
-            if ((double)D > m + (double)(A.eD_abs + A.eD_rel * (float)m)) continue;
-          }
-          tri_step64(A.rec[prim], p, m, proj, false);
-          have = true;
-          ++fp64;
-        } else {
-          if (sp >= kStack) { overflow = true; break; }
-          stack[sp++] = cs[q];
-        }
-      }
-      if (overflow) break;
+    } else {
+      ok = nearest(A, p, p32, INFINITY, m, proj, have, fp64);
     }
-    if (overflow) count_add(A.counters, C_ERR_STACK, 1);
+    if (!ok) count_add(A.counters, C_ERR_STACK, 1);
     A.dist[lin] = m;
     if (A.xp) {
       A.xp[3 * lin] = proj.x;
@@ -516,8 +537,16 @@ __global__ void __launch_bounds__(128) k_unbounded(UnbArgs A) {
       A.xp[3 * lin + 2] = proj.z;
     }
   }
-  for (int off = 16; off > 0; off >>= 1) fp64 += __shfl_down_sync(0xffffffffu, fp64, off);
-  if ((threadIdx.x & 31) == 0 && fp64) count_add(A.counters, C_FP64, fp64);
+  for (int off = 16; off > 0; off >>= 1) {
+    fp64 += __shfl_down_sync(0xffffffffu, fp64, off);
+    cert += __shfl_down_sync(0xffffffffu, cert, off);
+    fallback += __shfl_down_sync(0xffffffffu, fallback, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (fp64) count_add(A.counters, C_FP64, fp64);
+    if (cert) count_add(A.counters, C_CERTIFIED, cert);
+    if (fallback) count_add(A.counters, C_UNB_FALLBACK, fallback);
+  }
 }
 
 int ceil_log2(uint64_t v) {
@@ -546,8 +575,15 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
   const float pad = 2.0e-6f * E;
 
   if (mode == SDFGPU_MODE_UNBOUNDED) {
-    (void)use_learned;
-    UnbArgs A{g, nodes, leaf_prim, v32, rec, pad, eD_abs, eD_rel, 2 * nel + 64, d_dist, d_xp, ctx->d_counters};
+    float* radius = nullptr;
+    if (use_learned) {
+      // r = (dhat (1 + 0.1) + coarse spacing / s) s: a margin for the network's error and for
+      // the interpolation between the training nodes
+      SDF_TRY(scratch_t(ctx, "radius", (size_t)g.ngp, &radius));
+      const RadiusNorm& R = ctx->radius;
+      SDF_TRY(run_radius(ctx, &g, nullptr, g.ngp, 0.1f, (float)(R.coarse_h / R.s), radius));
+    }
+    UnbArgs A{g, nodes, leaf_prim, v32, rec, pad, eD_abs, eD_rel, 2 * nel + 64, radius, d_dist, d_xp, ctx->d_counters};
     SDF_MARK(ctx, T_TILES);
     k_unbounded<<<grid_for(g.ngp, 128, 148 * 32), 128, 0, st>>>(A);
     SDF_KERNEL(ctx);

@@ -48,7 +48,7 @@ class Stats(ctypes.Structure):
         ("ms_distance", ctypes.c_double), ("ms_sign", ctypes.c_double), ("ms_mesh", ctypes.c_double),
         ("launches", ctypes.c_int64), ("mesh_launches", ctypes.c_int64), ("ms_tiles", ctypes.c_double),
         ("ms_fold", ctypes.c_double), ("ms_rows", ctypes.c_double), ("ms_parity", ctypes.c_double),
-        ("ms_vote", ctypes.c_double),
+        ("ms_vote", ctypes.c_double), ("certified_nodes", ctypes.c_int64), ("radius_loss", ctypes.c_double),
     ]
 
     def as_dict(self):
@@ -77,6 +77,15 @@ SIGNATURES = {
                            ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "sdfgpu_distances_noalloc": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, _dp,
                                   ctypes.c_double, _i64p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "sdfgpu_train_radius": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
+                             ctypes.c_uint64, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
+    "sdfgpu_radius_param_count": ([], ctypes.c_int),
+    "sdfgpu_radius_params": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), _dp], ctypes.c_int),
+    "sdfgpu_set_radius_params": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), _dp], ctypes.c_int),
+    "sdfgpu_radius_eval": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int64,
+                            ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
+    "sdfgpu_mlp_train_eval": ([ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_float)] * 3 + [ctypes.c_int64]
+                              + [ctypes.POINTER(ctypes.c_float)] * 3, ctypes.c_int),
     "sdfgpu_get_stream": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "sdfgpu_get_stats": ([ctypes.c_void_p, ctypes.POINTER(Stats)], ctypes.c_int),
 }
@@ -218,6 +227,40 @@ class Context:
                                             int(bool(use_winding_fallback)), ctypes.c_void_p(sdf_ptr),
                                             ctypes.c_void_p(dist_ptr or None), ctypes.c_void_p(sign_ptr or None),
                                             ctypes.c_void_p(conf_ptr or None)))
+
+    # ---- learned search radius ----
+    def train_radius(self, coarse_n=64, steps=1500, batch=8192, lr=2e-3, seed=0):
+        loss = ctypes.c_float()
+        self._check(lib().sdfgpu_train_radius(self._p, int(coarse_n), int(steps), int(batch), float(lr), int(seed),
+                                              ctypes.byref(loss)))
+        return loss.value
+
+    def radius_params(self):
+        n = lib().sdfgpu_radius_param_count()
+        P = np.empty(n, np.float32); norm = np.empty(4)
+        self._check(lib().sdfgpu_radius_params(self._p, P.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), _d(norm)))
+        return P, norm
+
+    def set_radius_params(self, P, norm):
+        P = np.ascontiguousarray(P, np.float32); norm = np.ascontiguousarray(norm, np.float64)
+        self._check(lib().sdfgpu_set_radius_params(self._p, P.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), _d(norm)))
+
+    def radius_eval(self, xn):
+        xn = np.ascontiguousarray(xn, np.float32).reshape(-1, 3)
+        out = np.empty(xn.shape[0], np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        self._check(lib().sdfgpu_radius_eval(self._p, xn.ctypes.data_as(fp), xn.shape[0], out.ctypes.data_as(fp)))
+        return out
+
+    def mlp_train_eval(self, P, xn, target):
+        fp = ctypes.POINTER(ctypes.c_float)
+        P = np.ascontiguousarray(P, np.float32); xn = np.ascontiguousarray(xn, np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(target, np.float32)
+        dh = np.empty(xn.shape[0], np.float32); loss = np.empty(1, np.float32); grad = np.empty(P.shape[0], np.float32)
+        self._check(lib().sdfgpu_mlp_train_eval(self._p, P.ctypes.data_as(fp), xn.ctypes.data_as(fp), t.ctypes.data_as(fp),
+                                                xn.shape[0], dh.ctypes.data_as(fp), loss.ctypes.data_as(fp),
+                                                grad.ctypes.data_as(fp)))
+        return dh, float(loss[0]), grad
 
     def stats(self) -> dict:
         s = Stats()
