@@ -7,7 +7,8 @@ signs and sdf = dist .* sign for every grid node (sdfgpu_sdf_device).  The refer
 same work per call (KD-trees and BVH are built inside evalDistancesOnTriMesh and
 raycast_sign_detection).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload torus128|icosphere|...]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload torus128|icosphere|blobs256|gyroid320]
+    python bench.py --workload batch256 [--streams S]   # uneven batch of 256 meshes (sdfgpu_sdf_batch)
     python bench.py --impl reference ...   # the reference algorithm on the host cores
 
 Multi-GPU (torchrun, one rank per GPU): every rank computes its own copy of the workload (weak
@@ -204,6 +205,112 @@ def run_reference(args, rank, world):
     return 0
 
 
+def make_batch(name: str):
+    """Meshes and grids of an uneven batch: batch256 = 256 meshes, seed 3 (icospheres L2-6 and
+    8-32-blob marching-cubes meshes, 32..160 nodes on each grid's long axis); batchN = the first N."""
+    from stl2sdf import DataImport, _native, synthetic
+
+    count = int(name[len("batch"):] or 256)
+    items = []
+    for r in synthetic.uneven_batch(count, seed=3):
+        X, IEN = DataImport.roundtrip_float32(*synthetic.batch_mesh(r))
+        o, _, N, h, ngp = _native.grid_setup(X.min(0), X.max(0), r["K"] - 7, 3)
+        items.append((X, IEN, o, h, N))
+    desc = (f"{count} meshes, seed 3: even entries icospheres L2-6 (320-81920 tris), odd entries marching cubes of "
+            f"8-32 Gaussian blobs at 32-320 cells (log-uniform); K nodes on each grid's long axis, K in [32, 160]")
+    return items, desc
+
+
+def run_batch(args, rank, world, local):
+    """Uneven batch through sdfgpu_sdf_batch (host meshes in, host fields out), the meshes dealt to
+    ranks by LPT.  Timed by the host clock around the call (the batch spans several streams and
+    host threads), max over ranks."""
+    import numpy as np
+    import torch
+
+    from stl2sdf import _native, sharding
+
+    items, desc = make_batch(args.workload)
+    ngps = [int(np.prod(np.asarray(m[4]) + 1)) for m in items]
+    plan = sharding.lpt_assign([sharding.mesh_work(n, m[1].shape[0]) for n, m in zip(ngps, items)], world)
+    mine = [items[i] for i in plan[rank]]
+    ctx = _native.Context(local)
+    dist_on = world > 1
+    if dist_on:
+        import torch.distributed as tdist
+
+    def timed(k, **kw):
+        if dist_on:
+            tdist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        launches = 0
+        for _ in range(k):
+            ctx.sdf_batch(mine, **kw)
+            launches += ctx.stats()["launches"] + ctx.stats()["mesh_launches"]
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if dist_on:
+            tt = torch.tensor([dt], dtype=torch.float64, device=f"cuda:{local}")
+            tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
+            dt = float(tt.item())
+        return dt, launches
+
+    t_tune = time.perf_counter()
+    ctx.sdf_batch(mine, streams=args.streams, autotune=True)  # first call: autotuning + allocation
+    t_tune = time.perf_counter() - t_tune
+    for _ in range(args.warmup - 1):
+        ctx.sdf_batch(mine, streams=args.streams, autotune=True)
+    with ClockSampler(local) as clk:
+        dt, launches = timed(args.steps, streams=args.streams, autotune=True)
+    st = ctx.stats()
+    one, _ = timed(1, streams=1, autotune=False)  # same batch, one stream, default tile
+    total = sum(ngps)
+    value = total * args.steps / dt
+    line = {
+        "metric": METRIC, "value": value, "unit": "nodes/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "description": desc, "meshes": len(items), "ngp": total,
+                   "nel": int(sum(m[1].shape[0] for m in items)), "mode": "ref-rule", "streams": args.streams,
+                   "l2": "inputs larger than L2 (sum of all fields)",
+                   "step": "sdfgpu_sdf_batch over every mesh: upload, LBVH, distance, sign, combine, fields to host",
+                   "timing": "host clock around the call, barrier + device sync on both sides"},
+        "e2e": {"value": value, "unit": "nodes/s",
+                "h2d_bytes_per_step": int(sum(m[0].nbytes + m[1].nbytes for m in mine)),
+                "d2h_bytes_per_step": int(8 * sum(ngps[i] for i in plan[rank]))},
+        "gpu_launches": int(launches),
+        "single_stream_default_tile": {"value": total / one, "s": one},
+        "first_call_s": t_tune,
+        "stages_ms_summed": {k: st[k] for k in ("ms_mesh", "ms_tiles", "ms_fold", "ms_rows", "ms_parity", "ms_vote")},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        nthreads = oracle.max_threads()
+        rng = np.random.default_rng(42)
+        picks = list(range(0, len(items), max(1, len(items) // 32)))
+        t0, nodes_done = time.perf_counter(), 0
+        for i in picks:
+            X, IEN, o, h, N = items[i]
+            nodes = np.sort(rng.choice(ngps[i], size=min(256, ngps[i]), replace=False)).astype(np.int64)
+            oracle.distances(X, IEN, o, h, N, mode=0, nodes=nodes, nthreads=nthreads)
+            oracle.signs(X, IEN, o, h, N, nodes=nodes, nthreads=nthreads)
+            nodes_done += nodes.shape[0]
+        cdt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": nodes_done / cdt, "unit": "nodes/s", "cores": nthreads, "kind": "port",
+                                "sample": f"256 seeded nodes of each of {len(picks)} meshes (every "
+                                          f"{max(1, len(items) // 32)}th), distance+sign, {cdt:.1f} s"}
+    if dist_on:
+        tdist.barrier()
+        tdist.destroy_process_group()
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -214,6 +321,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=1 << 14)
+    ap.add_argument("--streams", type=int, default=8, help="batch workloads: worker streams")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -237,6 +345,8 @@ def main():
 
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
+    if args.workload.startswith("batch"):
+        return run_batch(args, rank, world, local)
     X, IEN, g, desc = make_workload(args.workload)
     ngp = g["ngp"]
     ctx = _native.Context(local)

@@ -155,6 +155,21 @@ int sdfgpu_sdf_device(sdfgpu_ctx* ctx, const double origin[3], double h, const i
                       double confidence_threshold, int32_t use_winding_fallback, double* d_sdf,
                       double* d_dist, double* d_sign, double* d_conf);
 
+/* z-slab of sdfgpu_sdf: only the z layers k0..k1 (0 <= k0 <= k1 <= N[2]) of the grid
+ * (origin, h, N), written as an (N[0]+1) x (N[1]+1) x (k1-k0+1) block, x fastest.  Every value
+ * equals the value of the same node in the full-grid call (nodes stay origin + h * global index),
+ * so slabs computed on different GPUs concatenate along z into the full field.  This is how a grid
+ * of more than 2^31-1 nodes is computed, and how z-slab sharding splits one grid across ranks. */
+int sdfgpu_sdf_slab(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], int64_t k0,
+                    int64_t k1, int32_t mode, int32_t min_rays, int32_t max_rays,
+                    double confidence_threshold, int32_t use_winding_fallback, double* sdf_out,
+                    double* dist_out, double* sign_out, double* conf_out);
+/* Same with device output pointers, as sdfgpu_sdf_device. */
+int sdfgpu_sdf_slab_device(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3],
+                           int64_t k0, int64_t k1, int32_t mode, int32_t min_rays, int32_t max_rays,
+                           double confidence_threshold, int32_t use_winding_fallback, double* d_sdf,
+                           double* d_dist, double* d_sign, double* d_conf);
+
 /* Allocation-free distances.  No counterpart in the reference: it exists for callers that must
  * not allocate GPU memory -- code running inside a host callback or an allocator hook, processes
  * whose device memory belongs to another framework's pool, or real-time loops that cannot take the
@@ -172,8 +187,45 @@ int sdfgpu_distances_noalloc(const double* d_X, int64_t nnp, const int64_t* d_IE
                              const double origin[3], double h, const int64_t N[3], int32_t mode,
                              double* d_dist_out, void* stream);
 
-/* Learned search radius for SDFGPU_MODE_UNBOUNDED (the north-star extension of the reference's
- * distance search; no reference counterpart).  A 3 x 64 Fourier-feature MLP (FP16 weights, FP32
+/* One mesh of a batch: the mesh (host X 3 x nnp, IEN 3 x nel 1-based), its grid (origin, h, N) and
+ * the host output buffer sdf (ngp doubles; dist/sign/conf optional, NULL to skip). */
+typedef struct sdfgpu_batch_item {
+  const double* X;
+  int64_t nnp;
+  const int64_t* IEN;
+  int64_t nel;
+  double origin[3];
+  double h;
+  int64_t N[3];
+  double* sdf;
+  double* dist;
+  double* sign;
+  double* conf;
+} sdfgpu_batch_item;
+
+/* stl_to_sdf's hot path (stl_to_sdf.jl:105-119) over many meshes, each with its own grid.  No
+ * single reference call does this; it is the batched form of sdfgpu_set_mesh + sdfgpu_sdf.
+ * `streams` worker contexts on the device of ctx (0 = 8), each with its own stream and host thread,
+ * take meshes from a shared queue, largest estimated work (ngp * log2(nel)) first, so small and
+ * large meshes overlap on the GPU.  With autotune = 1 each size class (log4 of ngp, log4 of nel)
+ * gets its tile from sdfgpu_autotune the first time it appears; the choice is kept in ctx for later
+ * calls.  Results equal per-mesh sdfgpu_sdf calls.  ctx's own mesh is left as it was; ctx's stats
+ * become the sums over the items (rho_max: the maximum; ms_*: summed per-item device times).
+ * Returns the first failure; its message names the item. */
+int sdfgpu_sdf_batch(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count, int32_t mode, int32_t min_rays,
+                     int32_t max_rays, double confidence_threshold, int32_t use_winding_fallback, int32_t streams,
+                     int32_t autotune);
+
+/* Tile autotuner for the distance stage (the reference has no counterpart).  Times the current mesh
+ * on the grid (origin, h, N) in `mode` with each built-in tile shape (nodes per CTA along x, y, z:
+ * 4x4x4, 8x4x2, 4x4x2, 8x4x4, 4x4x8, 8x8x4), keeps the fastest as ctx's tile and writes it to
+ * tile_out and its device time to ms_out (either may be NULL).  The tile changes only how the work
+ * is split, never a result. */
+int sdfgpu_autotune(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], int32_t mode,
+                    int32_t tile_out[3], double* ms_out);
+
+/* Learned search radius for SDFGPU_MODE_UNBOUNDED (an extension of the reference's distance
+ * search; no reference counterpart).  A 3 x 64 Fourier-feature MLP (FP16 weights, FP32
  * accumulate) is trained on the GPU on the exact unbounded distances of a coarse grid of the current
  * mesh (coarse_n nodes on its longest axis, Grid(Xmin, Xmax, coarse_n - 7, 3)).  sdfgpu_distances
  * with use_learned_radius = 1 then bounds each node's search by the predicted radius; a hit inside

@@ -1,0 +1,247 @@
+// batch.cu -- many meshes per call (sdfgpu_sdf_batch) and the tile autotuner (sdfgpu_autotune).
+//
+// A batch is a queue of (mesh, grid) items drained by worker contexts, one host thread and one
+// CUDA stream each.  The per-mesh pipeline has host-sized stages (the (tile, triangle) pair count,
+// the axis-row hit count, the undecided-node count), so one mesh alone leaves the GPU idle while
+// its host thread waits; several workers fill those gaps with the kernels of other meshes.  Items
+// are taken largest first (longest-processing-time order), which also makes each worker's scratch
+// buffers reach their final size on its first item, so later items allocate nothing.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <mutex>
+#include <numeric>
+#include <thread>
+
+#include "common.cuh"
+
+namespace sdfgpu {
+namespace {
+
+constexpr int32_t kTiles[][3] = {{4, 4, 4}, {8, 4, 2}, {4, 4, 2}, {8, 4, 4}, {4, 4, 8}, {8, 8, 4}};
+constexpr int kMaxStreams = 64;
+
+uint32_t pack_tile(const int32_t t[3]) { return (uint32_t)(t[0] | (t[1] << 8) | (t[2] << 16)); }
+void unpack_tile(uint32_t p, int32_t t[3]) {
+  t[0] = (int32_t)(p & 0xff);
+  t[1] = (int32_t)((p >> 8) & 0xff);
+  t[2] = (int32_t)((p >> 16) & 0xff);
+}
+
+int64_t item_ngp(const sdfgpu_batch_item& it) { return (it.N[0] + 1) * (it.N[1] + 1) * (it.N[2] + 1); }
+
+double item_work(const sdfgpu_batch_item& it) {
+  return (double)item_ngp(it) * std::log2(std::max(2.0, (double)it.nel));
+}
+
+// Size class of an item for the autotuner: floor(log4 ngp), floor(log4 nel).
+int64_t size_class(const sdfgpu_batch_item& it) {
+  auto lg4 = [](double v) { return (int64_t)std::floor(std::log2(std::max(1.0, v)) / 2.0); };
+  return lg4((double)item_ngp(it)) * 64 + lg4((double)it.nel);
+}
+
+void add_stats(sdfgpu_stats& a, const sdfgpu_stats& b) {
+  a.ngp += b.ngp;
+  a.nel += b.nel;
+  a.tile_pairs += b.tile_pairs;
+  a.active_tiles += b.active_tiles;
+  a.candidate_nodes += b.candidate_nodes;
+  a.fp64_evals += b.fp64_evals;
+  a.knn_fallback_nodes += b.knn_fallback_nodes;
+  a.band_nodes += b.band_nodes;
+  a.row_hits += b.row_hits;
+  a.undecided_nodes += b.undecided_nodes;
+  a.extra_rays += b.extra_rays;
+  a.winding_nodes += b.winding_nodes;
+  a.winding_ambiguous += b.winding_ambiguous;
+  a.unbounded_fallbacks += b.unbounded_fallbacks;
+  a.rho_max = std::max(a.rho_max, b.rho_max);
+  a.ms_distance += b.ms_distance;
+  a.ms_sign += b.ms_sign;
+  a.ms_mesh += b.ms_mesh;
+  a.launches += b.launches;
+  a.mesh_launches += b.mesh_launches;
+  a.ms_tiles += b.ms_tiles;
+  a.ms_fold += b.ms_fold;
+  a.ms_rows += b.ms_rows;
+  a.ms_parity += b.ms_parity;
+  a.ms_vote += b.ms_vote;
+  a.certified_nodes += b.certified_nodes;
+}
+
+struct BatchJob {
+  sdfgpu_ctx* parent;
+  sdfgpu_batch_item* items;
+  std::vector<int64_t> order;
+  int mode, min_rays, max_rays, use_winding, autotune;
+  double conf;
+  std::atomic<int64_t> next{0};
+  std::atomic<bool> stop{false};
+  std::mutex mu;  // guards rc, err, stats and parent->tuned
+  int rc = 0;
+  std::string err;
+  sdfgpu_stats stats = {};
+};
+
+}  // namespace
+
+// Times the distance stage of the current mesh on grid (origin, h, N) with every tile of kTiles.
+int autotune_tile(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], int mode, int32_t best[3],
+                  double* best_ms) {
+  const int32_t keep[3] = {ctx->tile[0], ctx->tile[1], ctx->tile[2]};
+  double best_t = 1e300;
+  int best_i = -1;
+  double* d_dist = nullptr;
+  for (int c = 0; c < (int)(sizeof(kTiles) / sizeof(kTiles[0])); ++c) {
+    for (int a = 0; a < 3; ++a) ctx->tile[a] = kTiles[c][a];
+    GridP g;
+    int rc = make_grid(ctx, origin, h, N, g);
+    if (rc == 0) rc = scratch_t(ctx, "out_dist", (size_t)g.ngp, &d_dist);
+    double t_min = 1e300;
+    for (int rep = 0; rep < 2 && rc == 0; ++rep) {
+      rc = reset_counters(ctx);
+      if (rc == 0 && cudaEventRecord(ctx->ev[0], ctx->stream) != cudaSuccess) rc = SDFGPU_ERR_CUDA;
+      if (rc == 0) rc = run_distances(ctx, g, mode, 0, d_dist, nullptr);
+      if (rc == 0 && cudaEventRecord(ctx->ev[1], ctx->stream) != cudaSuccess) rc = SDFGPU_ERR_CUDA;
+      if (rc == 0) rc = finish_counters(ctx, g);
+      float ms = 0.f;
+      if (rc == 0 && cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]) != cudaSuccess) rc = SDFGPU_ERR_CUDA;
+      if (rc == 0) t_min = std::min(t_min, (double)ms);
+    }
+    if (rc != 0) {
+      for (int a = 0; a < 3; ++a) ctx->tile[a] = keep[a];
+      if (ctx->err.empty()) ctx->err = "autotune: CUDA event failure";
+      return rc;
+    }
+    if (t_min < best_t) {
+      best_t = t_min;
+      best_i = c;
+    }
+  }
+  for (int a = 0; a < 3; ++a) ctx->tile[a] = best[a] = kTiles[best_i][a];
+  if (best_ms) *best_ms = best_t;
+  return 0;
+}
+
+namespace {
+
+int pick_tile(BatchJob& J, sdfgpu_ctx* w, const sdfgpu_batch_item& it) {
+  const int64_t key = size_class(it);
+  {
+    std::lock_guard<std::mutex> lk(J.mu);
+    auto f = J.parent->tuned.find(key);
+    if (f != J.parent->tuned.end()) {
+      unpack_tile(f->second, w->tile);
+      return 0;
+    }
+  }
+  int32_t t[3];
+  SDF_TRY(autotune_tile(w, it.origin, it.h, it.N, J.mode, t, nullptr));
+  std::lock_guard<std::mutex> lk(J.mu);
+  J.parent->tuned.emplace(key, pack_tile(t));  // a concurrent tuning of the same class may have won
+  return 0;
+}
+
+void worker_main(BatchJob& J, sdfgpu_ctx* w) {
+  const int64_t n = (int64_t)J.order.size();
+  for (;;) {
+    if (J.stop.load()) return;
+    const int64_t k = J.next.fetch_add(1);
+    if (k >= n) return;
+    const int64_t i = J.order[k];
+    sdfgpu_batch_item& it = J.items[i];
+    int rc = sdfgpu_set_mesh(w, it.X, it.nnp, it.IEN, it.nel);
+    sdfgpu_stats ms = w->stats;
+    if (rc == 0 && J.autotune) rc = pick_tile(J, w, it);
+    if (rc == 0)
+      rc = sdfgpu_sdf(w, it.origin, it.h, it.N, J.mode, J.min_rays, J.max_rays, J.conf, J.use_winding, it.sdf, it.dist,
+                      it.sign, it.conf);
+    std::lock_guard<std::mutex> lk(J.mu);
+    if (rc != 0) {
+      if (J.rc == 0) {
+        J.rc = rc;
+        J.err = "batch item " + std::to_string(i) + ": " + w->err;
+      }
+      J.stop.store(true);
+      return;
+    }
+    sdfgpu_stats s = w->stats;
+    s.ms_mesh = ms.ms_mesh;
+    s.mesh_launches = ms.mesh_launches;
+    add_stats(J.stats, s);
+  }
+}
+
+}  // namespace
+}  // namespace sdfgpu
+
+using namespace sdfgpu;
+
+extern "C" {
+
+int sdfgpu_autotune(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], int32_t mode,
+                    int32_t tile_out[3], double* ms_out) {
+  SDF_TRY(begin_call(ctx));
+  SDF_TRY(need_mesh(ctx));
+  SDF_TRY(check_mode(ctx, mode, 0));
+  int32_t t[3];
+  double ms = 0.0;
+  SDF_TRY(autotune_tile(ctx, origin, h, N, mode, t, &ms));
+  if (tile_out)
+    for (int a = 0; a < 3; ++a) tile_out[a] = t[a];
+  if (ms_out) *ms_out = ms;
+  return SDFGPU_OK;
+}
+
+int sdfgpu_sdf_batch(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count, int32_t mode, int32_t min_rays,
+                     int32_t max_rays, double confidence_threshold, int32_t use_winding_fallback, int32_t streams,
+                     int32_t autotune) {
+  SDF_TRY(begin_call(ctx));
+  if (count < 0 || (count > 0 && !items)) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "items must hold count entries");
+  if (streams < 0 || streams > kMaxStreams)
+    return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "streams must be in 0.." + std::to_string(kMaxStreams));
+  SDF_TRY(check_mode(ctx, mode, 0));
+  SDF_TRY(check_sign_args(ctx, min_rays, max_rays, confidence_threshold));
+  for (int64_t i = 0; i < count; ++i) {
+    const sdfgpu_batch_item& it = items[i];
+    if (!it.X || !it.IEN || !it.sdf || it.nnp < 1 || it.nel < 1)
+      return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "batch item " + std::to_string(i) + ": needs X, IEN, sdf and a non-empty mesh");
+  }
+  ctx->stats = sdfgpu_stats{};
+  if (count == 0) return SDFGPU_OK;
+  const int nw = (int)std::min<int64_t>(streams == 0 ? 8 : streams, count);
+  while ((int)ctx->workers.size() < nw) {
+    sdfgpu_opts o = {};
+    o.device = ctx->device;
+    for (int a = 0; a < 3; ++a) o.tile[a] = ctx->tile[a];
+    sdfgpu_ctx* w = nullptr;
+    if (sdfgpu_create(&o, &w) != SDFGPU_OK)
+      return fail(ctx, SDFGPU_ERR_CUDA, std::string("batch worker: ") + sdfgpu_last_error(nullptr));
+    ctx->workers.push_back(w);
+  }
+  BatchJob J;
+  J.parent = ctx;
+  J.items = items;
+  J.mode = mode;
+  J.min_rays = min_rays;
+  J.max_rays = max_rays;
+  J.conf = confidence_threshold;
+  J.use_winding = use_winding_fallback;
+  J.autotune = autotune;
+  J.order.resize((size_t)count);
+  std::iota(J.order.begin(), J.order.end(), (int64_t)0);
+  std::stable_sort(J.order.begin(), J.order.end(),
+                   [&](int64_t a, int64_t b) { return item_work(items[a]) > item_work(items[b]); });
+  for (int k = 0; k < nw; ++k)
+    if (!autotune)
+      for (int a = 0; a < 3; ++a) ctx->workers[k]->tile[a] = ctx->tile[a];
+  std::vector<std::thread> threads;
+  threads.reserve(nw);
+  for (int k = 0; k < nw; ++k) threads.emplace_back(worker_main, std::ref(J), ctx->workers[k]);
+  for (auto& t : threads) t.join();
+  ctx->stats = J.stats;
+  if (J.rc != 0) return fail(ctx, J.rc, J.err);
+  return SDFGPU_OK;
+}
+
+}  // extern "C"

@@ -121,22 +121,31 @@ int grid_core(const double xmin[3], const double xmax[3], int64_t n_max, int64_t
 
 }  // namespace
 
-int make_grid(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], GridP& g) {
+int make_grid(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], GridP& g, int64_t k0,
+              int64_t k1) {
   if (!origin || !N) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "origin and N must not be NULL");
   if (!(h > 0.0) || !std::isfinite(h)) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "cell size must be finite and > 0");
-  double ngp = 1.0;
   for (int a = 0; a < 3; ++a) {
     if (N[a] < 0) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "N must be >= 0");
     if (!std::isfinite(origin[a])) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "origin must be finite");
-    ngp *= (double)(N[a] + 1);
   }
+  if (k1 < 0) {
+    k0 = 0;
+    k1 = N[2];
+  }
+  if (k0 < 0 || k1 < k0 || k1 > N[2])
+    return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "z layers must satisfy 0 <= k0 <= k1 <= N[2]");
+  const int64_t nloc[3] = {N[0], N[1], k1 - k0};
+  double ngp = 1.0;
+  for (int a = 0; a < 3; ++a) ngp *= (double)(nloc[a] + 1);
   if (ngp > 2147483647.0)
-    return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "grid has more than 2^31-1 nodes (split it into slabs)");
+    return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "grid has more than 2^31-1 nodes (split it into z slabs)");
   const MeshDev& M = ctx->mesh;
+  g.k0 = k0;
   for (int a = 0; a < 3; ++a) {
     g.o[a] = origin[a];
-    g.N[a] = N[a];
-    g.n[a] = N[a] + 1;
+    g.N[a] = nloc[a];
+    g.n[a] = nloc[a] + 1;
     g.center[a] = M.center[a];
     g.t[a] = ctx->tile[a];
     g.nt[a] = cdiv(g.n[a], g.t[a]);
@@ -153,11 +162,7 @@ int make_grid(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N
   return 0;
 }
 
-}  // namespace sdfgpu
-
-using namespace sdfgpu;
-
-namespace {
+// ---- call scaffolding shared by the entry points here and in batch.cu -------------------------
 
 int begin_call(sdfgpu_ctx* ctx) {
   if (!ctx) return SDFGPU_ERR_INVALID_ARGUMENT;
@@ -259,7 +264,53 @@ int run_all(sdfgpu_ctx* ctx, const GridP& g, bool want_dist, bool want_sign, int
   return 0;
 }
 
-}  // namespace
+// The fused distance x sign over z layers k0..k1 of the grid (k1 < 0: every layer), device outputs.
+int sdf_device_impl(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], int64_t k0, int64_t k1,
+                    int mode, int min_rays, int max_rays, double conf, int use_winding, double* d_sdf, double* d_dist,
+                    double* d_sign, double* d_conf) {
+  SDF_TRY(begin_call(ctx));
+  SDF_TRY(need_mesh(ctx));
+  SDF_TRY(check_mode(ctx, mode, 0));
+  SDF_TRY(check_sign_args(ctx, min_rays, max_rays, conf));
+  if (!d_sdf) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "d_sdf must not be NULL");
+  GridP g;
+  SDF_TRY(make_grid(ctx, origin, h, N, g, k0, k1));
+  if (!d_dist) SDF_TRY(scratch_t(ctx, "out_dist", (size_t)g.ngp, &d_dist));
+  if (!d_sign) SDF_TRY(scratch_t(ctx, "out_sign", (size_t)g.ngp, &d_sign));
+  if (!d_conf) SDF_TRY(scratch_t(ctx, "out_conf", (size_t)g.ngp, &d_conf));
+  return run_all(ctx, g, true, true, mode, 0, min_rays, max_rays, conf, use_winding, d_dist, nullptr, d_sign, d_conf,
+                 d_sdf);
+}
+
+// Same, results copied to host buffers.
+int sdf_host_impl(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], int64_t k0, int64_t k1,
+                  int mode, int min_rays, int max_rays, double conf, int use_winding, double* sdf_out,
+                  double* dist_out, double* sign_out, double* conf_out) {
+  SDF_TRY(begin_call(ctx));
+  SDF_TRY(need_mesh(ctx));
+  if (!sdf_out) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "sdf_out must not be NULL");
+  GridP g;
+  SDF_TRY(make_grid(ctx, origin, h, N, g, k0, k1));
+  double *d_sdf, *d_dist, *d_sign, *d_conf;
+  SDF_TRY(scratch_t(ctx, "out_sdf", (size_t)g.ngp, &d_sdf));
+  SDF_TRY(scratch_t(ctx, "out_dist", (size_t)g.ngp, &d_dist));
+  SDF_TRY(scratch_t(ctx, "out_sign", (size_t)g.ngp, &d_sign));
+  SDF_TRY(scratch_t(ctx, "out_conf", (size_t)g.ngp, &d_conf));
+  SDF_TRY(sdf_device_impl(ctx, origin, h, N, k0, k1, mode, min_rays, max_rays, conf, use_winding, d_sdf, d_dist,
+                          d_sign, d_conf));
+  cudaStream_t st = ctx->stream;
+  const size_t bytes = sizeof(double) * g.ngp;
+  SDF_CUDA(ctx, cudaMemcpyAsync(sdf_out, d_sdf, bytes, cudaMemcpyDeviceToHost, st));
+  if (dist_out) SDF_CUDA(ctx, cudaMemcpyAsync(dist_out, d_dist, bytes, cudaMemcpyDeviceToHost, st));
+  if (sign_out) SDF_CUDA(ctx, cudaMemcpyAsync(sign_out, d_sign, bytes, cudaMemcpyDeviceToHost, st));
+  if (conf_out) SDF_CUDA(ctx, cudaMemcpyAsync(conf_out, d_conf, bytes, cudaMemcpyDeviceToHost, st));
+  SDF_CUDA(ctx, cudaStreamSynchronize(st));
+  return SDFGPU_OK;
+}
+
+}  // namespace sdfgpu
+
+using namespace sdfgpu;
 
 extern "C" {
 
@@ -322,6 +373,7 @@ int sdfgpu_create(const sdfgpu_opts* opts, sdfgpu_ctx** out) {
 
 int sdfgpu_destroy(sdfgpu_ctx* ctx) {
   if (!ctx) return SDFGPU_OK;
+  for (sdfgpu_ctx* w : ctx->workers) sdfgpu_destroy(w);
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (auto& kv : ctx->bufs)
@@ -411,43 +463,33 @@ int sdfgpu_signs(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_
 int sdfgpu_sdf_device(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], int32_t mode,
                       int32_t min_rays, int32_t max_rays, double confidence_threshold, int32_t use_winding_fallback,
                       double* d_sdf, double* d_dist, double* d_sign, double* d_conf) {
-  SDF_TRY(begin_call(ctx));
-  SDF_TRY(need_mesh(ctx));
-  SDF_TRY(check_mode(ctx, mode, 0));
-  SDF_TRY(check_sign_args(ctx, min_rays, max_rays, confidence_threshold));
-  if (!d_sdf) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "d_sdf must not be NULL");
-  GridP g;
-  SDF_TRY(make_grid(ctx, origin, h, N, g));
-  if (!d_dist) SDF_TRY(scratch_t(ctx, "out_dist", (size_t)g.ngp, &d_dist));
-  if (!d_sign) SDF_TRY(scratch_t(ctx, "out_sign", (size_t)g.ngp, &d_sign));
-  if (!d_conf) SDF_TRY(scratch_t(ctx, "out_conf", (size_t)g.ngp, &d_conf));
-  return run_all(ctx, g, true, true, mode, 0, min_rays, max_rays, confidence_threshold, use_winding_fallback, d_dist,
-                 nullptr, d_sign, d_conf, d_sdf);
+  return sdf_device_impl(ctx, origin, h, N, 0, -1, mode, min_rays, max_rays, confidence_threshold,
+                         use_winding_fallback, d_sdf, d_dist, d_sign, d_conf);
 }
 
 int sdfgpu_sdf(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], int32_t mode, int32_t min_rays,
                int32_t max_rays, double confidence_threshold, int32_t use_winding_fallback, double* sdf_out,
                double* dist_out, double* sign_out, double* conf_out) {
-  SDF_TRY(begin_call(ctx));
-  SDF_TRY(need_mesh(ctx));
-  if (!sdf_out) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "sdf_out must not be NULL");
-  GridP g;
-  SDF_TRY(make_grid(ctx, origin, h, N, g));
-  double *d_sdf, *d_dist, *d_sign, *d_conf;
-  SDF_TRY(scratch_t(ctx, "out_sdf", (size_t)g.ngp, &d_sdf));
-  SDF_TRY(scratch_t(ctx, "out_dist", (size_t)g.ngp, &d_dist));
-  SDF_TRY(scratch_t(ctx, "out_sign", (size_t)g.ngp, &d_sign));
-  SDF_TRY(scratch_t(ctx, "out_conf", (size_t)g.ngp, &d_conf));
-  SDF_TRY(sdfgpu_sdf_device(ctx, origin, h, N, mode, min_rays, max_rays, confidence_threshold, use_winding_fallback,
-                            d_sdf, d_dist, d_sign, d_conf));
-  cudaStream_t st = ctx->stream;
-  const size_t bytes = sizeof(double) * g.ngp;
-  SDF_CUDA(ctx, cudaMemcpyAsync(sdf_out, d_sdf, bytes, cudaMemcpyDeviceToHost, st));
-  if (dist_out) SDF_CUDA(ctx, cudaMemcpyAsync(dist_out, d_dist, bytes, cudaMemcpyDeviceToHost, st));
-  if (sign_out) SDF_CUDA(ctx, cudaMemcpyAsync(sign_out, d_sign, bytes, cudaMemcpyDeviceToHost, st));
-  if (conf_out) SDF_CUDA(ctx, cudaMemcpyAsync(conf_out, d_conf, bytes, cudaMemcpyDeviceToHost, st));
-  SDF_CUDA(ctx, cudaStreamSynchronize(st));
-  return SDFGPU_OK;
+  return sdf_host_impl(ctx, origin, h, N, 0, -1, mode, min_rays, max_rays, confidence_threshold, use_winding_fallback,
+                       sdf_out, dist_out, sign_out, conf_out);
+}
+
+int sdfgpu_sdf_slab(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], int64_t k0, int64_t k1,
+                    int32_t mode, int32_t min_rays, int32_t max_rays, double confidence_threshold,
+                    int32_t use_winding_fallback, double* sdf_out, double* dist_out, double* sign_out,
+                    double* conf_out) {
+  if (k1 < 0) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "z layers must satisfy 0 <= k0 <= k1 <= N[2]");
+  return sdf_host_impl(ctx, origin, h, N, k0, k1, mode, min_rays, max_rays, confidence_threshold,
+                       use_winding_fallback, sdf_out, dist_out, sign_out, conf_out);
+}
+
+int sdfgpu_sdf_slab_device(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], int64_t k0,
+                           int64_t k1, int32_t mode, int32_t min_rays, int32_t max_rays, double confidence_threshold,
+                           int32_t use_winding_fallback, double* d_sdf, double* d_dist, double* d_sign,
+                           double* d_conf) {
+  if (k1 < 0) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "z layers must satisfy 0 <= k0 <= k1 <= N[2]");
+  return sdf_device_impl(ctx, origin, h, N, k0, k1, mode, min_rays, max_rays, confidence_threshold,
+                         use_winding_fallback, d_sdf, d_dist, d_sign, d_conf);
 }
 
 int sdfgpu_train_radius(sdfgpu_ctx* ctx, int32_t coarse_n, int32_t steps, int32_t batch, float lr, uint64_t seed,

@@ -4,8 +4,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
 #include <string>
 #include <unordered_map>
+#include <vector>
 
 #include "exact64.cuh"
 #include "geom32.cuh"
@@ -59,7 +61,18 @@ struct GridP {
   int32_t t[3];     // tile dims (nodes)
   int64_t nt[3];    // tiles per axis
   int64_t ntiles;
+  int64_t k0 = 0;   // z index of local layer 0 in the full grid (a z-slab call), else 0
 };
+
+// Node (i, j, k) of the call in FP64, k local to the slab: origin + h * (global index), the
+// reference's mul-then-add (Grid.jl:90).
+__device__ __forceinline__ d3 gnode(const GridP& g, int64_t i, int64_t j, int64_t k) {
+  return node_coord(g.o, g.h, i, j, k + g.k0);
+}
+// Global index along axis a of local index idx.
+__host__ __device__ __forceinline__ int64_t gidx(const GridP& g, int a, int64_t idx) {
+  return a == 2 ? idx + g.k0 : idx;
+}
 
 struct MeshDev {
   int64_t nnp = 0, nel = 0;
@@ -92,6 +105,8 @@ struct sdfgpu_ctx {
   sdfgpu::RadiusNorm radius;  // learned search radius (radius.cu)
   int64_t launches = 0;  // kernels of this library launched since the last reset
   cudaEvent_t tev[8] = {};  // stage timestamps, see sdfgpu::Stage
+  std::vector<sdfgpu_ctx*> workers;      // batch workers (batch.cu), created on first use
+  std::map<int64_t, uint32_t> tuned;     // autotuner: size class -> packed tile (batch.cu)
 };
 
 namespace sdfgpu {
@@ -166,8 +181,22 @@ __device__ __forceinline__ void count_add(int64_t* counters, int idx, int64_t v)
   atomicAdd((unsigned long long*)&counters[idx], (unsigned long long)v);
 }
 
+// Call scaffolding of the entry points (capi.cu).
+int begin_call(sdfgpu_ctx* ctx);
+int need_mesh(sdfgpu_ctx* ctx);
+int reset_counters(sdfgpu_ctx* ctx);
+int finish_counters(sdfgpu_ctx* ctx, const GridP& g);
+int check_sign_args(sdfgpu_ctx* ctx, int min_rays, int max_rays, double conf);
+int check_mode(sdfgpu_ctx* ctx, int mode, int learned);
+int run_all(sdfgpu_ctx* ctx, const GridP& g, bool want_dist, bool want_sign, int mode, int learned, int min_rays,
+            int max_rays, double conf, int use_winding, double* d_dist, double* d_xp, double* d_sign, double* d_conf,
+            double* d_sdf);
+
 // Fills GridP from (origin, h, N) and the current mesh frame; validates sizes.
-int make_grid(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], GridP& g);
+// k0..k1 (inclusive, k1 >= 0) restricts the call to those z layers of the grid (a z-slab);
+// k1 < 0 means all layers.
+int make_grid(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], GridP& g, int64_t k0 = 0,
+              int64_t k1 = -1);
 
 // Stage entry points (implemented in mesh.cu / distance.cu / sign.cu).
 int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const int64_t* IEN, int64_t nel,

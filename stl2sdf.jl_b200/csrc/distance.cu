@@ -50,7 +50,8 @@ __device__ __forceinline__ float3 local32(const GridP& g, const d3& p) {
 
 // Index range [lo, hi] of the nodes whose coordinate along axis a can lie in [x0, x1].
 __device__ __forceinline__ bool axis_range(const GridP& g, int a, double x0, double x1, int64_t& lo, int64_t& hi) {
-  double f0 = (x0 - g.o[a]) / g.h - 1e-6, f1 = (x1 - g.o[a]) / g.h + 1e-6;
+  const double shift = (double)gidx(g, a, 0);
+  double f0 = (x0 - g.o[a]) / g.h - shift - 1e-6, f1 = (x1 - g.o[a]) / g.h - shift + 1e-6;
   f0 = fmax(f0, -1.0);
   f1 = fmin(f1, (double)g.N[a] + 1.0);
   if (!(f0 <= f1)) return false;
@@ -100,7 +101,8 @@ __global__ void k_tile_pairs(const double4* __restrict__ cent, const TriRec64* _
               double s = 0.0;
               for (int a = 0; a < 3; ++a) {
                 const double c = 0.5 * (lo[a] + hi[a]);
-                const double b0 = g.o[a] + g.h * (double)ia[a], b1 = g.o[a] + g.h * (double)ib[a];
+                const double b0 = g.o[a] + g.h * (double)gidx(g, a, ia[a]);
+                const double b1 = g.o[a] + g.h * (double)gidx(g, a, ib[a]);
                 const double d = c < b0 ? b0 - c : (c > b1 ? c - b1 : 0.0);
                 s += d * d;
               }
@@ -172,8 +174,8 @@ __global__ void __launch_bounds__(256) k_tile_fold(FoldArgs A) {
   const int64_t i = tx * g.t[0] + lx, j = ty * g.t[1] + ly, k = tz * g.t[2] + lz;
   const bool valid = i <= g.N[0] && j <= g.N[1] && k <= g.N[2];
   const int64_t lin = i + g.n[0] * (j + g.n[1] * k);
-  const d3 p = node_coord(g.o, g.h, i, j, k);
-  const d3 t0 = node_coord(g.o, g.h, tx * g.t[0], ty * g.t[1], tz * g.t[2]);
+  const d3 p = gnode(g, i, j, k);
+  const d3 t0 = gnode(g, tx * g.t[0], ty * g.t[1], tz * g.t[2]);
   const float3 pl = make_float3((float)(p.x - t0.x), (float)(p.y - t0.y), (float)(p.z - t0.z));
   const float plen = len3(pl);
   const float sr = (float)(2.5 * g.h);
@@ -313,7 +315,7 @@ __global__ void k_band(const float4* __restrict__ v32, const TriRec64* __restric
     for (int64_t k = lo[2]; k <= hi[2]; ++k)
       for (int64_t j = lo[1]; j <= hi[1]; ++j)
         for (int64_t i = lo[0]; i <= hi[0]; ++i) {
-          const d3 p = node_coord(g.o, g.h, i, j, k);
+          const d3 p = gnode(g, i, j, k);
           if (pt_tri_d2(local32(g, p), a, b, c) <= hb2) band[i + g.n[0] * (j + g.n[1] * k)] = 1;
         }
   }
@@ -360,7 +362,7 @@ __global__ void k_knn_fallback(KnnArgs A) {
     if (A.band && !A.band[lin]) continue;
     int64_t i, j, k;
     node_ijk(g, lin, i, j, k);
-    const d3 p = node_coord(g.o, g.h, i, j, k);
+    const d3 p = gnode(g, i, j, k);
     const float3 p32 = local32(g, p);
     double bs[3] = {INFINITY, INFINITY, INFINITY};
     int64_t bv[3] = {-1, -1, -1};
@@ -511,7 +513,7 @@ __global__ void __launch_bounds__(128) k_unbounded(UnbArgs A) {
   for (int64_t lin = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; lin < g.ngp; lin += (int64_t)gridDim.x * blockDim.x) {
     int64_t i, j, k;
     node_ijk(g, lin, i, j, k);
-    const d3 p = node_coord(g.o, g.h, i, j, k);
+    const d3 p = gnode(g, i, j, k);
     const float3 p32 = local32(g, p);
     double m = kBig;
     d3 proj = {0.0, 0.0, 0.0};
@@ -654,6 +656,8 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
   if (g.ntiles > 0x7fffffffLL) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "grid has too many tiles");
   SDF_MARK(ctx, T_TILES);
   const size_t smem = sizeof(WarpStage) * (size_t)(threads / 32);
+  if (smem > 48 * 1024)  // tiles of more than 5 warps stage more than the default 48 KB
+    SDF_CUDA(ctx, cudaFuncSetAttribute(k_tile_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_tile_fold<<<(unsigned)g.ntiles, threads, smem, st>>>(A);
   SDF_KERNEL(ctx);
   SDF_MARK(ctx, T_FOLD);

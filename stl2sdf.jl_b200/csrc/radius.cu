@@ -193,7 +193,7 @@ __global__ void k_make_samples(const double* __restrict__ dist, GridP g, double 
                                float* __restrict__ X, float* __restrict__ T) {
   for (int64_t lin = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; lin < g.ngp; lin += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = lin % g.n[0], j = (lin / g.n[0]) % g.n[1], k = lin / (g.n[0] * g.n[1]);
-    const d3 p = node_coord(g.o, g.h, i, j, k);
+    const d3 p = gnode(g, i, j, k);
     X[3 * lin] = (float)((p.x - cx) / s);
     X[3 * lin + 1] = (float)((p.y - cy) / s);
     X[3 * lin + 2] = (float)((p.z - cz) / s);

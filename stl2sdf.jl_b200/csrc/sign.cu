@@ -103,7 +103,8 @@ __device__ __forceinline__ bool row_test(const TriRec64& r, double ob, double oc
 }
 
 __device__ __forceinline__ bool axis_range2(const GridP& g, int a, double x0, double x1, int64_t& lo, int64_t& hi) {
-  double f0 = (x0 - g.o[a]) / g.h - 1e-6, f1 = (x1 - g.o[a]) / g.h + 1e-6;
+  const double shift = (double)gidx(g, a, 0);
+  double f0 = (x0 - g.o[a]) / g.h - shift - 1e-6, f1 = (x1 - g.o[a]) / g.h - shift + 1e-6;
   f0 = fmax(f0, -1.0);
   f1 = fmin(f1, (double)g.N[a] + 1.0);
   if (!(f0 <= f1)) return false;
@@ -123,9 +124,9 @@ __device__ __forceinline__ void tri_rows(const GridP& g, const TriRec64& r, bool
   if (!axis_range2(g, b, r.bmin[b], r.bmax[b], b0, b1)) return;
   if (!axis_range2(g, c, r.bmin[c], r.bmax[c], c0, c1)) return;
   for (int64_t jc = c0; jc <= c1; ++jc) {
-    const double oc = da(g.o[c], dm(g.h, (double)jc));
+    const double oc = da(g.o[c], dm(g.h, (double)gidx(g, c, jc)));
     for (int64_t jb = b0; jb <= b1; ++jb) {
-      const double ob = da(g.o[b], dm(g.h, (double)jb));
+      const double ob = da(g.o[b], dm(g.h, (double)gidx(g, b, jb)));
       const int64_t row = row_base + jc * g.n[b] + jb;
       if (!fill) {
         if (row_test<AX>(r, ob, oc, nullptr)) { atomicAdd(&row_cnt[row], 1); ++nhit; }
@@ -209,7 +210,7 @@ __global__ void __launch_bounds__(256) k_axis_parity(GridP g, int64_t row_base, 
     const int64_t row = row_base + jc * g.n[b] + jb;
     const int32_t off = row_off[row], n = row_cnt[row];
     if (n > kRowCap) { par[lin] = 0x80; continue; }
-    const double xa = da(g.o[AX], dm(g.h, (double)ia));
+    const double xa = da(g.o[AX], dm(g.h, (double)gidx(g, AX, ia)));
     double ts[kRowCap];
     for (int q = 0; q < n; ++q) {
       const double tv = row_t<AX>(hits[off + q], xa);
@@ -475,7 +476,7 @@ __global__ void __launch_bounds__(128) k_rays(RayArgs A, int round) {
     const int r = A.req_ray[t];
     const int64_t lin = A.list[q];
     const int64_t i = lin % g.n[0], j = (lin / g.n[0]) % g.n[1], k = lin / (g.n[0] * g.n[1]);
-    const d3 p = node_coord(g.o, g.h, i, j, k);
+    const d3 p = gnode(g, i, j, k);
     const float3 p32 = make_float3((float)(p.x - g.center[0]), (float)(p.y - g.center[1]), (float)(p.z - g.center[2]));
     int v = ray_parity(A, p, p32, r - 1);
     if (v < 0) { count_add(A.counters, C_ERR_CAPACITY, 1); v = 0; }
@@ -501,7 +502,7 @@ __global__ void __launch_bounds__(256) k_winding(GridP g, const TriRec64* __rest
   for (int64_t q = blockIdx.y; q < count; q += gridDim.y) {
     const int64_t lin = list[q];
     const int64_t i = lin % g.n[0], j = (lin / g.n[0]) % g.n[1], k = lin / (g.n[0] * g.n[1]);
-    const d3 p = node_coord(g.o, g.h, i, j, k);
+    const d3 p = gnode(g, i, j, k);
     double w = 0.0;
     const int64_t e1 = min((int64_t)(chunk + 1) * kWindChunk, nel);
     for (int64_t el = (int64_t)chunk * kWindChunk + threadIdx.x; el < e1; el += blockDim.x) {

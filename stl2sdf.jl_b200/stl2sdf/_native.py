@@ -55,6 +55,14 @@ class Stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BatchItem(ctypes.Structure):
+    _fields_ = [
+        ("X", _dp), ("nnp", ctypes.c_int64), ("IEN", _i64p), ("nel", ctypes.c_int64),
+        ("origin", ctypes.c_double * 3), ("h", ctypes.c_double), ("N", ctypes.c_int64 * 3),
+        ("sdf", _dp), ("dist", _dp), ("sign", _dp), ("conf", _dp),
+    ]
+
+
 # Every symbol include/sdfgpu.h declares, with its ctypes signature.
 SIGNATURES = {
     "sdfgpu_abi_version": ([], ctypes.c_int),
@@ -75,6 +83,12 @@ SIGNATURES = {
     "sdfgpu_sdf_device": ([ctypes.c_void_p, _dp, ctypes.c_double, _i64p, ctypes.c_int32, ctypes.c_int32,
                            ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                            ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "sdfgpu_sdf_slab": ([ctypes.c_void_p, _dp, ctypes.c_double, _i64p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32,
+                         ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _dp, _dp, _dp, _dp],
+                        ctypes.c_int),
+    "sdfgpu_sdf_slab_device": ([ctypes.c_void_p, _dp, ctypes.c_double, _i64p, ctypes.c_int64, ctypes.c_int64,
+                                ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
+                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "sdfgpu_distances_noalloc": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, _dp,
                                   ctypes.c_double, _i64p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "sdfgpu_train_radius": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
@@ -86,6 +100,11 @@ SIGNATURES = {
                             ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
     "sdfgpu_mlp_train_eval": ([ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_float)] * 3 + [ctypes.c_int64]
                               + [ctypes.POINTER(ctypes.c_float)] * 3, ctypes.c_int),
+    "sdfgpu_sdf_batch": ([ctypes.c_void_p, ctypes.POINTER(BatchItem), ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
+                          ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32],
+                         ctypes.c_int),
+    "sdfgpu_autotune": ([ctypes.c_void_p, _dp, ctypes.c_double, _i64p, ctypes.c_int32,
+                         ctypes.POINTER(ctypes.c_int32), _dp], ctypes.c_int),
     "sdfgpu_get_stream": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "sdfgpu_get_stats": ([ctypes.c_void_p, ctypes.POINTER(Stats)], ctypes.c_int),
 }
@@ -227,6 +246,64 @@ class Context:
                                             int(bool(use_winding_fallback)), ctypes.c_void_p(sdf_ptr),
                                             ctypes.c_void_p(dist_ptr or None), ctypes.c_void_p(sign_ptr or None),
                                             ctypes.c_void_p(conf_ptr or None)))
+
+    def sdf_slab(self, origin, h, N, k0, k1, mode=MODE_REF_RULE, min_rays=6, max_rays=30, confidence_threshold=0.6,
+                 use_winding_fallback=True, want_parts=False):
+        """z layers k0..k1 of the grid (origin, h, N): an (N0+1)(N1+1)(k1-k0+1) block, x fastest."""
+        N = np.ascontiguousarray(N, np.int64)
+        origin = np.ascontiguousarray(origin, np.float64)
+        n = int((N[0] + 1) * (N[1] + 1) * (int(k1) - int(k0) + 1))
+        sdf = np.empty(max(n, 0))
+        parts = [np.empty(max(n, 0)) for _ in range(3)] if want_parts else [None, None, None]
+        self._check(lib().sdfgpu_sdf_slab(self._p, _d(origin), float(h), _i(N), int(k0), int(k1), int(mode),
+                                          int(min_rays), int(max_rays), float(confidence_threshold),
+                                          int(bool(use_winding_fallback)), _d(sdf),
+                                          *[(_d(p) if p is not None else None) for p in parts]))
+        return (sdf, *parts) if want_parts else sdf
+
+    def sdf_slab_device(self, origin, h, N, k0, k1, sdf_ptr, mode=MODE_REF_RULE, min_rays=6, max_rays=30,
+                        confidence_threshold=0.6, use_winding_fallback=True, dist_ptr=0, sign_ptr=0, conf_ptr=0):
+        N = np.ascontiguousarray(N, np.int64)
+        origin = np.ascontiguousarray(origin, np.float64)
+        self._check(lib().sdfgpu_sdf_slab_device(self._p, _d(origin), float(h), _i(N), int(k0), int(k1), int(mode),
+                                                 int(min_rays), int(max_rays), float(confidence_threshold),
+                                                 int(bool(use_winding_fallback)), ctypes.c_void_p(sdf_ptr),
+                                                 ctypes.c_void_p(dist_ptr or None), ctypes.c_void_p(sign_ptr or None),
+                                                 ctypes.c_void_p(conf_ptr or None)))
+
+    def sdf_batch(self, meshes, mode=MODE_REF_RULE, min_rays=6, max_rays=30, confidence_threshold=0.6,
+                  use_winding_fallback=True, streams=8, autotune=True, want_parts=False):
+        """SDFs of many meshes, each on its own grid: meshes = [(X, IEN, origin, h, N), ...].
+        Returns one sdf array per mesh (with want_parts, (sdf, dist, sign, conf) per mesh)."""
+        keep, outs = [], []
+        items = (BatchItem * max(1, len(meshes)))()
+        for k, (X, IEN, origin, h, N) in enumerate(meshes):
+            X = np.ascontiguousarray(X, np.float64).reshape(-1, 3)
+            IEN = np.ascontiguousarray(IEN, np.int64).reshape(-1, 3)
+            N = np.ascontiguousarray(N, np.int64)
+            ngp = int(np.prod(N + 1))
+            out = [np.empty(ngp)] + ([np.empty(ngp) for _ in range(3)] if want_parts else [None] * 3)
+            keep += [X, IEN]
+            outs.append(out)
+            it = items[k]
+            it.X, it.nnp, it.IEN, it.nel = _d(X), X.shape[0], _i(IEN), IEN.shape[0]
+            it.origin[:] = [float(v) for v in origin]
+            it.h = float(h)
+            it.N[:] = [int(v) for v in N]
+            it.sdf, it.dist, it.sign, it.conf = [(_d(a) if a is not None else None) for a in out]
+        self._check(lib().sdfgpu_sdf_batch(self._p, items, len(meshes), int(mode), int(min_rays), int(max_rays),
+                                           float(confidence_threshold), int(bool(use_winding_fallback)),
+                                           int(streams), int(bool(autotune))))
+        return [tuple(o) if want_parts else o[0] for o in outs]
+
+    def autotune(self, origin, h, N, mode=MODE_REF_RULE):
+        """Picks the fastest tile for the current mesh on this grid; returns (tile, ms)."""
+        N = np.ascontiguousarray(N, np.int64)
+        origin = np.ascontiguousarray(origin, np.float64)
+        tile = (ctypes.c_int32 * 3)()
+        ms = ctypes.c_double(0.0)
+        self._check(lib().sdfgpu_autotune(self._p, _d(origin), float(h), _i(N), int(mode), tile, ctypes.byref(ms)))
+        return tuple(tile), ms.value
 
     # ---- learned search radius ----
     def train_radius(self, coarse_n=64, steps=1500, batch=8192, lr=2e-3, seed=0):

@@ -183,6 +183,33 @@ def gyroid(cells: int = 384, thickness: float = 0.04, periods: float = 2.0):
     return _collect(h)
 
 
+def uneven_batch(count: int = 256, seed: int = 3, k_lo: int = 32, k_hi: int = 160):
+    """Recipes of an uneven batch of meshes from numpy's default_rng(seed): the even entries are
+    icospheres of level 2..6 (320..81,920 triangles, radial jitter N(0, 0.01)), the odd entries
+    marching-cubes meshes of 8..32 Gaussian blobs extracted at 32..320 cells per axis (log-uniform;
+    about 1k..400k triangles).  Each gets its own grid with K nodes on the longest axis, K uniform
+    in [k_lo, k_hi].  Returns a list of dicts (kind, level | nblobs/cells/seed, K); `batch_mesh`
+    builds one."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        K = int(rng.integers(k_lo, k_hi + 1))
+        if i % 2 == 0:
+            out.append(dict(kind="icosphere", level=int(rng.integers(2, 7)), seed=int(rng.integers(1 << 30)), K=K))
+        else:
+            cells = int(round(32.0 * 10.0 ** rng.uniform(0.0, 1.0)))
+            out.append(dict(kind="blobs", nblobs=int(rng.integers(8, 33)), cells=cells,
+                            seed=int(rng.integers(1 << 30)), K=K))
+    return out
+
+
+def batch_mesh(recipe: dict):
+    """(V, F) of one `uneven_batch` entry (before the float32 STL round trip)."""
+    if recipe["kind"] == "icosphere":
+        return icosphere(recipe["level"], jitter=0.01, seed=recipe["seed"])
+    return blobs(recipe["nblobs"], seed=recipe["seed"], cells=recipe["cells"])
+
+
 def mc_table():
     """The derived marching-cubes table: (256, 16, 3) edge ids (-1 padded), (12, 2) edge corners."""
     import ctypes

@@ -1,0 +1,97 @@
+"""Uneven batch (many meshes, each on its own grid, one call) and the tile autotuner.
+
+The batch must give, per mesh, exactly what one sdfgpu_set_mesh + sdfgpu_sdf call gives with the
+default tile; the autotuner may change the tile, never a result.  A few batch nodes are also
+checked against the oracle directly.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import sample_nodes
+
+pytestmark = pytest.mark.gpu
+
+
+def _batch(count, seed, k_lo, k_hi):
+    from stl2sdf import DataImport, _native, synthetic
+
+    out = []
+    for r in synthetic.uneven_batch(count, seed=seed, k_lo=k_lo, k_hi=k_hi):
+        if r["kind"] == "blobs":
+            r["cells"] = min(r["cells"], 96)  # keep the oracle checks below quick
+        X, IEN = DataImport.roundtrip_float32(*synthetic.batch_mesh(r))
+        o, _, N, h, _ = _native.grid_setup(X.min(0), X.max(0), r["K"] - 7, 3)
+        out.append((X, IEN, o, h, N))
+    return out
+
+
+@pytest.fixture(scope="module")
+def small_batch():
+    return _batch(12, seed=3, k_lo=24, k_hi=56)
+
+
+def test_batch_equals_single_calls(gpu_ctx, small_batch):
+    got = gpu_ctx.sdf_batch(small_batch, streams=4, autotune=True, want_parts=True)
+    st = gpu_ctx.stats()
+    assert st["ngp"] == sum(int(np.prod(np.asarray(m[4]) + 1)) for m in small_batch)
+    for (X, IEN, o, h, N), parts in zip(small_batch, got):
+        gpu_ctx.set_mesh(X, IEN)
+        want = gpu_ctx.sdf(o, h, N, want_parts=True)
+        for a, b in zip(parts, want):
+            assert np.array_equal(a, b)
+    # a second call reuses the workers and the tuned tiles
+    again = gpu_ctx.sdf_batch(small_batch, streams=3, autotune=True)
+    for a, parts in zip(again, got):
+        assert np.array_equal(a, parts[0])
+
+
+def test_batch_matches_oracle(gpu_ctx, small_batch):
+    picks = sorted(range(len(small_batch)), key=lambda k: small_batch[k][1].shape[0])[:3]
+    sub = [small_batch[k] for k in picks]
+    got = gpu_ctx.sdf_batch(sub, streams=2, autotune=False, want_parts=True)
+    for (X, IEN, o, h, N), (sdf, dist, sign, conf) in zip(sub, got):
+        nodes = sample_nodes(sdf.shape[0], 1500, seed=11)
+        d_ref, _, _ = oracle.distances(X, IEN, o, h, N, mode=0, nodes=nodes)
+        r = oracle.signs(X, IEN, o, h, N, nodes=nodes)
+        s_ref, c_ref = r["sign"], r["conf"]
+        assert np.array_equal(dist[nodes], d_ref)
+        assert np.array_equal(sign[nodes], s_ref)
+        assert np.array_equal(conf[nodes], c_ref)
+        assert np.array_equal(sdf[nodes], d_ref * s_ref)
+
+
+def test_autotune_keeps_results(gpu_ctx, torus_mesh):
+    from conftest import grid_of
+
+    X, IEN = torus_mesh
+    g = grid_of(X, n_nodes_long_axis=64)
+    gpu_ctx.set_mesh(X, IEN)
+    base, _ = gpu_ctx.distances(g["origin"], g["h"], g["N"], 0)
+    tile, ms = gpu_ctx.autotune(g["origin"], g["h"], g["N"], 0)
+    assert tile in [(4, 4, 4), (8, 4, 2), (4, 4, 2), (8, 4, 4), (4, 4, 8), (8, 8, 4)] and ms > 0
+    tuned, _ = gpu_ctx.distances(g["origin"], g["h"], g["N"], 0)
+    assert np.array_equal(base, tuned)
+    for t in [(8, 8, 4), (4, 4, 2), (8, 4, 2)]:  # every shape, not only the winner, gives the same field
+        from stl2sdf import _native
+
+        c = _native.Context(0, tile=t)
+        c.set_mesh(X, IEN)
+        d, _ = c.distances(g["origin"], g["h"], g["N"], 0)
+        c.close()
+        assert np.array_equal(base, d), t
+
+
+def test_batch_reports_failing_item(gpu_ctx, small_batch):
+    from stl2sdf import _native
+
+    bad = list(small_batch[:3])
+    X, IEN, o, h, N = bad[1]
+    bad[1] = (X, IEN, o, -1.0, N)
+    with pytest.raises(_native.SdfGpuError) as e:
+        gpu_ctx.sdf_batch(bad, streams=2)
+    assert "batch item 1" in str(e.value)
+    assert gpu_ctx.sdf_batch([], streams=2) == []
