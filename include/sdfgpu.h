@@ -102,6 +102,7 @@ typedef struct sdfgpu_stats {
   double ms_vote;                 /* vote + adaptive rays + winding */
   int64_t certified_nodes;        /* learned radius: nodes whose bounded search certified the result */
   double radius_loss;             /* final training loss of the radius network */
+  int64_t bvh_visits;             /* LBVH nodes visited by the unbounded search (one per warp and node) */
 } sdfgpu_stats;
 
 /* Context lifetime.  opts may be NULL (device 0, default tiles). */
@@ -219,8 +220,10 @@ int sdfgpu_sdf_batch(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count, i
 /* Tile autotuner for the distance stage (the reference has no counterpart).  Times the current mesh
  * on the grid (origin, h, N) in `mode` with each built-in tile shape (nodes per CTA along x, y, z:
  * 4x4x4, 8x4x2, 4x4x2, 8x4x4, 4x4x8, 8x8x4), keeps the fastest as ctx's tile and writes it to
- * tile_out and its device time to ms_out (either may be NULL).  The tile changes only how the work
- * is split, never a result. */
+ * tile_out and its device time to ms_out (either may be NULL).  In SDFGPU_MODE_UNBOUNDED, which
+ * has no tiles, it times the warp bricks instead (the 32 nodes one warp searches together:
+ * 4x2x4, 4x4x2, 2x4x4, 8x4x1, 4x8x1, 32x1x1) and keeps the fastest as ctx's brick.  Neither shape
+ * changes a result, only how the work is split. */
 int sdfgpu_autotune(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], int32_t mode,
                     int32_t tile_out[3], double* ms_out);
 
@@ -233,6 +236,13 @@ int sdfgpu_autotune(sdfgpu_ctx* ctx, const double origin[3], double h, const int
  * unbounded_fallbacks).  Results are bit-identical to the plain unbounded mode. */
 int sdfgpu_train_radius(sdfgpu_ctx* ctx, int32_t coarse_n, int32_t steps, int32_t batch, float lr, uint64_t seed,
                         float* final_loss);
+/* Warp brick of the unbounded search: the nodes (brick[0] x brick[1] x brick[2] along x, y, z,
+ * product 32) whose nearest triangles one warp searches together.  Default 4 x 2 x 4. */
+int sdfgpu_set_brick(sdfgpu_ctx* ctx, const int32_t brick[3]);
+/* Margin of the learned radius: r = (dhat (1 + alpha) + beta * coarse spacing / s) * s, where dhat is
+ * the network's normalised distance and s its normalisation scale.  Defaults alpha = 0.1, beta = 1.
+ * A smaller margin prunes more and certifies fewer nodes; results never change. */
+int sdfgpu_set_radius_margin(sdfgpu_ctx* ctx, float alpha, float beta);
 /* Number of FP32 parameters of the radius network (layout: W1 64x32, b1, W2 64x64, b2, W3 64x64,
  * b3, w4 64, b4). */
 int sdfgpu_radius_param_count(void);

@@ -19,6 +19,8 @@ namespace sdfgpu {
 namespace {
 
 constexpr int32_t kTiles[][3] = {{4, 4, 4}, {8, 4, 2}, {4, 4, 2}, {8, 4, 4}, {4, 4, 8}, {8, 8, 4}};
+// Warp bricks (nodes of one warp) of the unbounded search.
+constexpr int32_t kBricks[][3] = {{4, 2, 4}, {4, 4, 2}, {2, 4, 4}, {8, 4, 1}, {4, 8, 1}, {32, 1, 1}};
 constexpr int kMaxStreams = 64;
 
 uint32_t pack_tile(const int32_t t[3]) { return (uint32_t)(t[0] | (t[1] << 8) | (t[2] << 16)); }
@@ -67,6 +69,7 @@ void add_stats(sdfgpu_stats& a, const sdfgpu_stats& b) {
   a.ms_parity += b.ms_parity;
   a.ms_vote += b.ms_vote;
   a.certified_nodes += b.certified_nodes;
+  a.bvh_visits += b.bvh_visits;
 }
 
 struct BatchJob {
@@ -85,15 +88,20 @@ struct BatchJob {
 
 }  // namespace
 
-// Times the distance stage of the current mesh on grid (origin, h, N) with every tile of kTiles.
+// Times the distance stage of the current mesh on grid (origin, h, N) with every tile of kTiles, or,
+// in the unbounded mode (which has no tiles), with every warp brick of kBricks.
 int autotune_tile(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], int mode, int32_t best[3],
                   double* best_ms) {
-  const int32_t keep[3] = {ctx->tile[0], ctx->tile[1], ctx->tile[2]};
+  const bool bricks = mode == SDFGPU_MODE_UNBOUNDED;
+  int32_t* shape = bricks ? ctx->brick : ctx->tile;
+  const int32_t(*table)[3] = bricks ? kBricks : kTiles;
+  const int count = bricks ? (int)(sizeof(kBricks) / sizeof(kBricks[0])) : (int)(sizeof(kTiles) / sizeof(kTiles[0]));
+  const int32_t keep[3] = {shape[0], shape[1], shape[2]};
   double best_t = 1e300;
   int best_i = -1;
   double* d_dist = nullptr;
-  for (int c = 0; c < (int)(sizeof(kTiles) / sizeof(kTiles[0])); ++c) {
-    for (int a = 0; a < 3; ++a) ctx->tile[a] = kTiles[c][a];
+  for (int c = 0; c < count; ++c) {
+    for (int a = 0; a < 3; ++a) shape[a] = table[c][a];
     GridP g;
     int rc = make_grid(ctx, origin, h, N, g);
     if (rc == 0) rc = scratch_t(ctx, "out_dist", (size_t)g.ngp, &d_dist);
@@ -109,7 +117,7 @@ int autotune_tile(sdfgpu_ctx* ctx, const double origin[3], double h, const int64
       if (rc == 0) t_min = std::min(t_min, (double)ms);
     }
     if (rc != 0) {
-      for (int a = 0; a < 3; ++a) ctx->tile[a] = keep[a];
+      for (int a = 0; a < 3; ++a) shape[a] = keep[a];
       if (ctx->err.empty()) ctx->err = "autotune: CUDA event failure";
       return rc;
     }
@@ -118,7 +126,7 @@ int autotune_tile(sdfgpu_ctx* ctx, const double origin[3], double h, const int64
       best_i = c;
     }
   }
-  for (int a = 0; a < 3; ++a) ctx->tile[a] = best[a] = kTiles[best_i][a];
+  for (int a = 0; a < 3; ++a) shape[a] = best[a] = table[best_i][a];
   if (best_ms) *best_ms = best_t;
   return 0;
 }
@@ -131,7 +139,7 @@ int pick_tile(BatchJob& J, sdfgpu_ctx* w, const sdfgpu_batch_item& it) {
     std::lock_guard<std::mutex> lk(J.mu);
     auto f = J.parent->tuned.find(key);
     if (f != J.parent->tuned.end()) {
-      unpack_tile(f->second, w->tile);
+      unpack_tile(f->second, J.mode == SDFGPU_MODE_UNBOUNDED ? w->brick : w->tile);
       return 0;
     }
   }
@@ -234,7 +242,10 @@ int sdfgpu_sdf_batch(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count, i
                    [&](int64_t a, int64_t b) { return item_work(items[a]) > item_work(items[b]); });
   for (int k = 0; k < nw; ++k)
     if (!autotune)
-      for (int a = 0; a < 3; ++a) ctx->workers[k]->tile[a] = ctx->tile[a];
+      for (int a = 0; a < 3; ++a) {
+        ctx->workers[k]->tile[a] = ctx->tile[a];
+        ctx->workers[k]->brick[a] = ctx->brick[a];
+      }
   std::vector<std::thread> threads;
   threads.reserve(nw);
   for (int k = 0; k < nw; ++k) threads.emplace_back(worker_main, std::ref(J), ctx->workers[k]);

@@ -205,6 +205,7 @@ int finish_counters(sdfgpu_ctx* ctx, const GridP& g) {
   s.unbounded_fallbacks = c[C_UNB_FALLBACK];
   s.rho_max = ctx->mesh.rho_max;
   s.certified_nodes = c[C_CERTIFIED];
+  s.bvh_visits = c[C_VISITS];
   s.radius_loss = ctx->radius.loss;
   if (c[C_ERR_STACK]) return fail(ctx, SDFGPU_ERR_CAPACITY, "BVH traversal stack overflow");
   if (c[C_ERR_CAPACITY])
@@ -514,6 +515,23 @@ int sdfgpu_set_radius_params(sdfgpu_ctx* ctx, const float* params, const double 
   SDF_TRY(begin_call(ctx));
   if (!params || !norm || !(norm[3] > 0.0)) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "bad params or norm");
   return set_radius_params(ctx, params, norm);
+}
+
+int sdfgpu_set_radius_margin(sdfgpu_ctx* ctx, float alpha, float beta) {
+  SDF_TRY(begin_call(ctx));
+  if (!(alpha >= 0.f && alpha <= 10.f) || !(beta >= 0.f && beta <= 100.f))
+    return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "radius margin: need 0 <= alpha <= 10 and 0 <= beta <= 100");
+  ctx->radius.alpha = alpha;
+  ctx->radius.beta = beta;
+  return SDFGPU_OK;
+}
+
+int sdfgpu_set_brick(sdfgpu_ctx* ctx, const int32_t brick[3]) {
+  SDF_TRY(begin_call(ctx));
+  if (!brick || brick[0] < 1 || brick[1] < 1 || brick[2] < 1 || brick[0] * brick[1] * brick[2] != 32)
+    return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "brick: three positive extents whose product is 32");
+  for (int a = 0; a < 3; ++a) ctx->brick[a] = brick[a];
+  return SDFGPU_OK;
 }
 
 int sdfgpu_radius_eval(sdfgpu_ctx* ctx, const float* xn, int64_t B, float* dhat) {

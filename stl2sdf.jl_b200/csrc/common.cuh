@@ -46,6 +46,7 @@ enum Counter : int {
   C_LIST_UNDECIDED, // length of the undecided-node list
   C_LIST_WINDING,   // length of the winding list
   C_CERTIFIED,      // learned radius: nodes certified by the bounded search
+  C_VISITS,         // LBVH nodes visited by the unbounded search
   C_NUM = 32
 };
 
@@ -96,6 +97,7 @@ struct sdfgpu_ctx {
   cudaEvent_t ev[6] = {};
   std::string err;
   int32_t tile[3] = {4, 4, 4};
+  int32_t brick[3] = {4, 2, 4};  // nodes of one warp in the unbounded search (product 32)
   bool has_mesh = false;
   sdfgpu::MeshDev mesh;
   std::unordered_map<std::string, sdfgpu::DevBuf> bufs;

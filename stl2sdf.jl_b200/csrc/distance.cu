@@ -443,6 +443,10 @@ __global__ void k_knn_fallback(KnnArgs A) {
   if ((threadIdx.x & 31) == 0 && done) count_add(A.counters, C_KNN, done);
 }
 
+constexpr int kUnbWarps = 8;     // warps per CTA of k_unbounded
+constexpr int kWarpStack = 64;   // per-warp traversal stack (shared memory)
+constexpr int kKeep = 8;         // per-lane triangles kept inside the FP32 band of the minimum
+
 struct UnbArgs {
   GridP g;
   const BNode* nodes;
@@ -456,87 +460,210 @@ struct UnbArgs {
   double* dist;
   double* xp;
   int64_t* counters;
+  int32_t b[3];         // brick of one warp: nodes along x, y, z (product 32)
+  int64_t nb[3];        // bricks per axis
+  int64_t nbricks;
 };
 
-// Depth-first LBVH nearest search from node p, nearer child first.  Boxes farther than the bound
-// (the running minimum plus the FP32 margin, or `r0` before the first hit) are pruned; candidates
-// inside the FP32 error band of the running minimum get the FP64 reference step (true minimum).
-// Returns false when a visit or stack bound is exceeded.
-__device__ bool nearest(const UnbArgs& A, const d3& p, const float3& p32, float r0, double& m, d3& proj, bool& have,
-                        int64_t& fp64) {
-  int stack[kStack];
-  int sp = 0;
-  stack[sp++] = 0;
+// The FP64 step out of line: it is rare on this path, and inlining it would size the registers of
+// the whole traversal loop for it.
+__device__ __noinline__ void step64_call(const TriRec64* rec, int prim, const d3& p, double& m64, d3& proj) {
+  tri_step64(rec[prim], p, m64, proj, false);
+}
+
+// Per-lane state of the FP32 search: the smallest FP32 point-triangle distance m (INF before the
+// first hit) and the triangles whose FP32 distance lies within band(m) = m + 2 err(m), one of
+// which is the true (FP64) nearest: |FP32 - FP64| <= err for every distance, so the FP64 winner t*
+// has D32(t*) <= d64(t*) + err <= d64(t_m) + err <= m + 2 err.  Slots hold INF when free.
+struct LaneBest {
+  float m;
+  bool overflow;  // the band held more than kKeep triangles at some point
+  int t[kKeep];
+  float d[kKeep];
+};
+
+__device__ __forceinline__ float band_of(const UnbArgs& A, float m) { return m + 2.f * (A.eD_abs + A.eD_rel * m); }
+
+__device__ __forceinline__ void lane_offer(const UnbArgs& A, LaneBest& L, float D, int tri) {
+  if (D < L.m) {
+    L.m = D;
+    const float bd = band_of(A, D);
+#pragma unroll
+    for (int q = 0; q < kKeep; ++q)
+      if (L.d[q] > bd) L.d[q] = INFINITY;
+  } else if (D > band_of(A, L.m)) {
+    return;
+  }
+  bool placed = false;
+#pragma unroll
+  for (int q = 0; q < kKeep; ++q)
+    if (L.d[q] != INFINITY && L.t[q] == tri) placed = true;  // already kept (a second pass)
+#pragma unroll
+  for (int q = 0; q < kKeep; ++q)
+    if (!placed && L.d[q] == INFINITY) {
+      L.d[q] = D;
+      L.t[q] = tri;
+      placed = true;
+    }
+  if (!placed) L.overflow = true;
+}
+
+// One warp searches the LBVH for the nearest triangles of its 32 nodes together (a packet
+// traversal).  The stack is the warp's, in shared memory; a child is visited when its box lies
+// within the bound of at least one active lane -- band(m) of the lane's FP32 minimum, or r0 before
+// its first hit -- nearer child first as seen from the brick's central lane `rep`.  Every load of
+// a node or triangle is the same address for the whole warp.  kExact: every leaf triangle within a
+// lane's bound runs the FP64 step at once (used with a tight r0 for lanes whose band overflowed);
+// otherwise leaves only feed the lane's FP32 band.  Returns false when the visit or stack bound is
+// exceeded.
+template <bool kExact>
+__device__ bool warp_search(const UnbArgs& A, int* stack, int lane, int rep, const d3& p, const float3& p32,
+                            bool active, float r0, LaneBest& L, double& m64, d3& proj, int64_t& fp64,
+                            int64_t& visits_out) {
+  int sp = 1;
+  if (lane == 0) stack[0] = 0;
+  __syncwarp();
   int64_t visits = 0;
+  bool ok = true;
   while (sp > 0) {
-    if (++visits > A.max_visits) return false;
-    const BNode nd = A.nodes[stack[--sp]];
-    const float bound = have ? (float)m + A.eD_abs + A.eD_rel * (float)m + A.pad : r0 + A.pad;
+    if (++visits > A.max_visits) { ok = false; break; }
+    const int nid = stack[--sp];
+    __syncwarp();
+    const BNode nd = A.nodes[nid];
     float3 lo0, hi0, lo1, hi1;
     child_box(nd, 0, lo0, hi0);
     child_box(nd, 1, lo1, hi1);
-    float d0 = lo0.x > hi0.x ? INFINITY : box_d2(p32, lo0, hi0);
-    float d1 = lo1.x > hi1.x ? INFINITY : box_d2(p32, lo1, hi1);
-    const float b2 = bound * bound;
-    int c0 = nd.d.x, c1 = nd.d.y;
-    if (d1 < d0) {  // visit the nearer child first: push it last
-      float t = d0; d0 = d1; d1 = t;
-      int c = c0; c0 = c1; c1 = c;
+    const bool e0 = lo0.x > hi0.x, e1 = lo1.x > hi1.x;  // empty child
+    const float d0 = box_d2(p32, lo0, hi0), d1 = box_d2(p32, lo1, hi1);
+    float lim;
+    if (kExact) {
+      const float mf = (float)m64;
+      lim = fminf(r0, mf + A.eD_abs + A.eD_rel * mf);
+    } else {
+      lim = L.m < INFINITY ? band_of(A, L.m) : r0 + A.eD_abs + A.eD_rel * r0;
     }
-    const int cs[2] = {c1, c0};
-    const float ds2[2] = {d1, d0};
-    for (int q = 0; q < 2; ++q) {
-      if (isinf(ds2[q]) || !(ds2[q] <= b2)) continue;
-      if (cs[q] & kLeafBit) {
-        const int prim = A.leaf_prim[cs[q] & 0x7fffffff];
-        const float D = sqrtf(pt_tri_d2(p32, f3(A.v32[3 * prim]), f3(A.v32[3 * prim + 1]), f3(A.v32[3 * prim + 2])));
-        if (have && (double)D > m + (double)(A.eD_abs + A.eD_rel * (float)m)) continue;
-        if (!have && D > r0 + A.eD_abs + A.eD_rel * r0) continue;
-        tri_step64(A.rec[prim], p, m, proj, false);
-        have = true;
-        ++fp64;
+    const float b = lim + A.pad;
+    const float b2 = b * b;
+    const bool w0 = active && !e0 && d0 <= b2, w1 = active && !e1 && d1 <= b2;
+    const unsigned m0 = __ballot_sync(0xffffffffu, w0), m1 = __ballot_sync(0xffffffffu, w1);
+    const float rd0 = __shfl_sync(0xffffffffu, e0 ? INFINITY : d0, rep);
+    const float rd1 = __shfl_sync(0xffffffffu, e1 ? INFINITY : d1, rep);
+    const bool swap = rd1 < rd0;
+    const int cn = swap ? nd.d.y : nd.d.x, cf = swap ? nd.d.x : nd.d.y;
+    const unsigned mn = swap ? m1 : m0, mfar = swap ? m0 : m1;
+    const bool wn = swap ? w1 : w0, wf = swap ? w0 : w1;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {  // leaves now, near one first
+      const int c = q == 0 ? cn : cf;
+      const bool want = q == 0 ? wn : wf;
+      if (!(c & kLeafBit) || (q == 0 ? mn : mfar) == 0u) continue;
+      const int prim = A.leaf_prim[c & 0x7fffffff];
+      const float D = sqrtf(pt_tri_d2(p32, f3(A.v32[3 * prim]), f3(A.v32[3 * prim + 1]), f3(A.v32[3 * prim + 2])));
+      if (kExact) {
+        const float mf = (float)m64;
+        if (want && D <= fminf(r0, mf + A.eD_abs + A.eD_rel * mf)) {
+          step64_call(A.rec, prim, p, m64, proj);
+          ++fp64;
+        }
       } else {
-        if (sp >= kStack) return false;
-        stack[sp++] = cs[q];
+        const float limq = L.m < INFINITY ? band_of(A, L.m) : r0 + A.eD_abs + A.eD_rel * r0;
+        if (want && D <= limq) lane_offer(A, L, D, prim);
       }
     }
+    // inner children, the far one pushed first so the near one is popped next
+    if (mfar != 0u && !(cf & kLeafBit)) {
+      if (sp >= kWarpStack) { ok = false; break; }
+      if (lane == 0) stack[sp] = cf;
+      ++sp;
+    }
+    if (mn != 0u && !(cn & kLeafBit)) {
+      if (sp >= kWarpStack) { ok = false; break; }
+      if (lane == 0) stack[sp] = cn;
+      ++sp;
+    }
+    __syncwarp();
   }
-  return true;
+  __syncwarp();
+  visits_out += visits;
+  return ok;
 }
 
-// True nearest triangle of every node (no clamp).  With a learned radius r the first search is
-// bounded by r; a hit with d <= r is certified exact (every nearer triangle lies within r and was
-// visited), otherwise the node searches again without the bound.
-__global__ void __launch_bounds__(128) k_unbounded(UnbArgs A) {
+// FP64 steps over the kept triangles inside the final band, in ascending triangle index (so exact
+// ties keep the lowest index, as a fold in index order does).
+__device__ __forceinline__ void lane_resolve(const UnbArgs& A, const LaneBest& L, const d3& p, double& m64, d3& proj,
+                                             int64_t& fp64) {
+  const float bd = band_of(A, L.m);
+  int last = -1;
+#pragma unroll 1
+  for (int it = 0; it < kKeep; ++it) {
+    int best = 0x7fffffff;
+#pragma unroll
+    for (int q = 0; q < kKeep; ++q)
+      if (L.d[q] <= bd && L.t[q] > last && L.t[q] < best) best = L.t[q];
+    if (best == 0x7fffffff) break;
+    step64_call(A.rec, best, p, m64, proj);
+    ++fp64;
+    last = best;
+  }
+}
+
+// True nearest triangle of every node (no clamp), one warp per brick of 32 nodes.  With a learned
+// radius r the first search of each lane is bounded by r; a minimum certainly <= r is exact (every
+// nearer triangle lies within r and was visited), and the lanes without one search again without
+// the bound, keeping what they found.  Lanes whose band overflowed search once more with FP64
+// steps bounded by the band.
+__global__ void __launch_bounds__(kUnbWarps * 32, 2) k_unbounded(UnbArgs A) {
+  __shared__ int s_stack[kUnbWarps][kWarpStack];
   const GridP& g = A.g;
-  int64_t fp64 = 0, cert = 0, fallback = 0;
-  for (int64_t lin = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; lin < g.ngp; lin += (int64_t)gridDim.x * blockDim.x) {
-    int64_t i, j, k;
-    node_ijk(g, lin, i, j, k);
-    const d3 p = gnode(g, i, j, k);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int* stack = s_stack[w];
+  const int lx = lane % A.b[0], ly = (lane / A.b[0]) % A.b[1], lz = lane / (A.b[0] * A.b[1]);
+  const int rep = A.b[0] / 2 + A.b[0] * (A.b[1] / 2 + A.b[1] * (A.b[2] / 2));
+  int64_t fp64 = 0, cert = 0, fallback = 0, errs = 0, visits = 0;
+  for (int64_t brick = (int64_t)blockIdx.x * kUnbWarps + w; brick < A.nbricks;
+       brick += (int64_t)gridDim.x * kUnbWarps) {
+    const int64_t bx = brick % A.nb[0], by = (brick / A.nb[0]) % A.nb[1], bz = brick / (A.nb[0] * A.nb[1]);
+    const int64_t i = bx * A.b[0] + lx, j = by * A.b[1] + ly, k = bz * A.b[2] + lz;
+    const bool valid = i <= g.N[0] && j <= g.N[1] && k <= g.N[2];
+    // lanes past the grid edge stand on the nearest grid node (they only order the traversal)
+    const d3 p = gnode(g, min(i, g.N[0]), min(j, g.N[1]), min(k, g.N[2]));
     const float3 p32 = local32(g, p);
-    double m = kBig;
+    const int64_t lin = i + g.n[0] * (j + g.n[1] * k);
+    LaneBest L;
+    L.m = INFINITY;
+    L.overflow = false;
+#pragma unroll
+    for (int q = 0; q < kKeep; ++q) {
+      L.t[q] = -1;
+      L.d[q] = INFINITY;
+    }
+    double m64 = kBig;
     d3 proj = {0.0, 0.0, 0.0};
-    bool have = false;
     bool ok;
     if (A.radius) {
-      const float r = A.radius[lin];
-      ok = nearest(A, p, p32, r, m, proj, have, fp64);
-      if (ok && have && m <= (double)r) {
-        ++cert;
-      } else if (ok) {
-        ++fallback;
-        ok = nearest(A, p, p32, INFINITY, m, proj, have, fp64);
-      }
+      const float r = valid ? A.radius[lin] : 0.f;
+      ok = warp_search<false>(A, stack, lane, rep, p, p32, valid, r, L, m64, proj, fp64, visits);
+      const bool certified = valid && L.m < INFINITY && L.m + A.eD_abs + A.eD_rel * L.m <= r;
+      if (valid && certified) ++cert;
+      if (valid && !certified) ++fallback;
+      if (ok && __any_sync(0xffffffffu, valid && !certified))
+        ok = warp_search<false>(A, stack, lane, rep, p, p32, valid && !certified, INFINITY, L, m64, proj, fp64,
+                                visits);
     } else {
-      ok = nearest(A, p, p32, INFINITY, m, proj, have, fp64);
+      ok = warp_search<false>(A, stack, lane, rep, p, p32, valid, INFINITY, L, m64, proj, fp64, visits);
     }
-    if (!ok) count_add(A.counters, C_ERR_STACK, 1);
-    A.dist[lin] = m;
-    if (A.xp) {
-      A.xp[3 * lin] = proj.x;
-      A.xp[3 * lin + 1] = proj.y;
-      A.xp[3 * lin + 2] = proj.z;
+    const bool over = valid && L.overflow;
+    if (ok && __any_sync(0xffffffffu, over))
+      ok = warp_search<true>(A, stack, lane, rep, p, p32, over, band_of(A, L.m), L, m64, proj, fp64, visits);
+    if (valid && !over) lane_resolve(A, L, p, m64, proj, fp64);
+    if (!ok && lane == 0) ++errs;
+    if (valid) {
+      A.dist[lin] = m64;
+      if (A.xp) {
+        A.xp[3 * lin] = proj.x;
+        A.xp[3 * lin + 1] = proj.y;
+        A.xp[3 * lin + 2] = proj.z;
+      }
     }
   }
   for (int off = 16; off > 0; off >>= 1) {
@@ -544,10 +671,12 @@ __global__ void __launch_bounds__(128) k_unbounded(UnbArgs A) {
     cert += __shfl_down_sync(0xffffffffu, cert, off);
     fallback += __shfl_down_sync(0xffffffffu, fallback, off);
   }
-  if ((threadIdx.x & 31) == 0) {
+  if (lane == 0) {
     if (fp64) count_add(A.counters, C_FP64, fp64);
     if (cert) count_add(A.counters, C_CERTIFIED, cert);
     if (fallback) count_add(A.counters, C_UNB_FALLBACK, fallback);
+    if (errs) count_add(A.counters, C_ERR_STACK, errs);
+    if (visits) count_add(A.counters, C_VISITS, visits);
   }
 }
 
@@ -579,15 +708,21 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
   if (mode == SDFGPU_MODE_UNBOUNDED) {
     float* radius = nullptr;
     if (use_learned) {
-      // r = (dhat (1 + 0.1) + coarse spacing / s) s: a margin for the network's error and for
-      // the interpolation between the training nodes
+      // r = (dhat (1 + alpha) + beta * coarse spacing / s) s: a margin for the network's error and
+      // for the interpolation between the training nodes
       SDF_TRY(scratch_t(ctx, "radius", (size_t)g.ngp, &radius));
       const RadiusNorm& R = ctx->radius;
-      SDF_TRY(run_radius(ctx, &g, nullptr, g.ngp, 0.1f, (float)(R.coarse_h / R.s), radius));
+      SDF_TRY(run_radius(ctx, &g, nullptr, g.ngp, R.alpha, (float)(R.beta * R.coarse_h / R.s), radius));
     }
     UnbArgs A{g, nodes, leaf_prim, v32, rec, pad, eD_abs, eD_rel, 2 * nel + 64, radius, d_dist, d_xp, ctx->d_counters};
+    A.nbricks = 1;
+    for (int a = 0; a < 3; ++a) {
+      A.b[a] = ctx->brick[a];
+      A.nb[a] = cdiv(g.n[a], A.b[a]);
+      A.nbricks *= A.nb[a];
+    }
     SDF_MARK(ctx, T_TILES);
-    k_unbounded<<<grid_for(g.ngp, 128, 148 * 32), 128, 0, st>>>(A);
+    k_unbounded<<<grid_for(A.nbricks, kUnbWarps, 148 * 8), kUnbWarps * 32, 0, st>>>(A);
     SDF_KERNEL(ctx);
     SDF_MARK(ctx, T_FOLD);
     return 0;

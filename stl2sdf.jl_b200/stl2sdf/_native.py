@@ -49,6 +49,7 @@ class Stats(ctypes.Structure):
         ("launches", ctypes.c_int64), ("mesh_launches", ctypes.c_int64), ("ms_tiles", ctypes.c_double),
         ("ms_fold", ctypes.c_double), ("ms_rows", ctypes.c_double), ("ms_parity", ctypes.c_double),
         ("ms_vote", ctypes.c_double), ("certified_nodes", ctypes.c_int64), ("radius_loss", ctypes.c_double),
+        ("bvh_visits", ctypes.c_int64),
     ]
 
     def as_dict(self):
@@ -105,6 +106,8 @@ SIGNATURES = {
                          ctypes.c_int),
     "sdfgpu_autotune": ([ctypes.c_void_p, _dp, ctypes.c_double, _i64p, ctypes.c_int32,
                          ctypes.POINTER(ctypes.c_int32), _dp], ctypes.c_int),
+    "sdfgpu_set_brick": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
+    "sdfgpu_set_radius_margin": ([ctypes.c_void_p, ctypes.c_float, ctypes.c_float], ctypes.c_int),
     "sdfgpu_get_stream": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "sdfgpu_get_stats": ([ctypes.c_void_p, ctypes.POINTER(Stats)], ctypes.c_int),
 }
@@ -305,7 +308,16 @@ class Context:
         self._check(lib().sdfgpu_autotune(self._p, _d(origin), float(h), _i(N), int(mode), tile, ctypes.byref(ms)))
         return tuple(tile), ms.value
 
+    def set_brick(self, brick):
+        """Nodes (x, y, z; product 32) one warp searches together in the unbounded mode."""
+        b = (ctypes.c_int32 * 3)(*[int(v) for v in brick])
+        self._check(lib().sdfgpu_set_brick(self._p, b))
+
     # ---- learned search radius ----
+    def set_radius_margin(self, alpha=0.1, beta=1.0):
+        """r = (dhat (1 + alpha) + beta * coarse spacing / s) * s."""
+        self._check(lib().sdfgpu_set_radius_margin(self._p, float(alpha), float(beta)))
+
     def train_radius(self, coarse_n=64, steps=1500, batch=8192, lr=2e-3, seed=0):
         loss = ctypes.c_float()
         self._check(lib().sdfgpu_train_radius(self._p, int(coarse_n), int(steps), int(batch), float(lr), int(seed),

@@ -268,3 +268,43 @@ def test_blobs_full_size_sample(gpu_ctx):
     check_dist(dist[nodes], dr, X)
     ref = oracle.signs(X, IEN, g["origin"], g["h"], g["N"], nodes=nodes)
     assert np.array_equal(sign[nodes], ref["sign"]) and np.array_equal(conf[nodes], ref["conf"])
+
+
+def _bipyramid(k=24):
+    """Closed double fan: two apexes shared by k triangles each (a vertex far above the number of
+    triangles the unbounded search keeps per node in its FP32 band, so nodes on the axis take
+    the exact re-search)."""
+    ang = 2 * np.pi * np.arange(k) / k
+    V = np.concatenate([[[0.0, 0.0, 1.0], [0.0, 0.0, -1.0]], np.stack([np.cos(ang), np.sin(ang), np.zeros(k)], 1)])
+    F = []
+    for q in range(k):
+        a, b = 2 + q, 2 + (q + 1) % k
+        F.append([0, a, b])
+        F.append([1, b, a])
+    return V, np.asarray(F)
+
+
+@pytest.mark.parametrize("brick", [(4, 2, 4), (32, 1, 1)])
+def test_unbounded_high_valence_vertex(gpu_ctx, brick):
+    from stl2sdf import DataImport
+
+    X, IEN = DataImport.roundtrip_float32(*_bipyramid())
+    g = grid_of(X, cell=0.1)
+    gpu_ctx.set_brick(brick)
+    try:
+        d, dr, _, _, _ = run_pair(gpu_ctx, X, IEN, g, mode=2)
+    finally:
+        gpu_ctx.set_brick((4, 2, 4))
+    check_dist(d, dr, X)
+
+
+def test_unbounded_brick_autotune(gpu_ctx, icosphere_mesh):
+    X, IEN = icosphere_mesh
+    g = grid_of(X, cell=0.05)
+    gpu_ctx.set_mesh(X, IEN)
+    d0, _ = gpu_ctx.distances(g["origin"], g["h"], g["N"], 2)
+    brick, ms = gpu_ctx.autotune(g["origin"], g["h"], g["N"], mode=2)
+    assert int(np.prod(brick)) == 32 and ms > 0
+    d1, _ = gpu_ctx.distances(g["origin"], g["h"], g["N"], 2)
+    gpu_ctx.set_brick((4, 2, 4))
+    assert np.array_equal(d0, d1)
