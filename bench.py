@@ -156,7 +156,10 @@ def distance_variants(ctx, X, IEN, g, reps=3):
 
     out["ref_rule"] = run(0)
     out["exact_h_bounded"] = run(1)
+    brick, _ = ctx.autotune(g["origin"], g["h"], g["N"], mode=2)  # the plain search at its best brick
     out["plain_unbounded"] = run(2)
+    out["plain_unbounded"].update({"brick": list(brick), "bvh_visits_per_node": ctx.stats()["bvh_visits"] / g["ngp"],
+                                   "fp64_steps_per_node": ctx.stats()["fp64_evals"] / g["ngp"]})
     t0 = _t.perf_counter()
     loss = ctx.train_radius(coarse_n=64, steps=1500, batch=8192)
     train_s = _t.perf_counter() - t0
@@ -164,7 +167,9 @@ def distance_variants(ctx, X, IEN, g, reps=3):
     st = ctx.stats()
     out["learned_unbounded"].update({"certified_fraction": st["certified_nodes"] / g["ngp"],
                                      "fallback_nodes": st["unbounded_fallbacks"], "train_s": train_s,
-                                     "train_loss": loss, "train_grid": "64 nodes on the long axis, 1500 Adam steps"})
+                                     "train_loss": loss, "train_grid": "64 nodes on the long axis, 1500 Adam steps",
+                                     "margin": "r = (dhat (1 + 0.1) + 1 coarse spacing) s",
+                                     "bvh_visits_per_node": st["bvh_visits"] / g["ngp"]})
     out["learned_vs_plain_unbounded"] = out["plain_unbounded"]["ms"] / out["learned_unbounded"]["ms"]
     return out
 
@@ -314,7 +319,8 @@ def run_batch(args, rank, world, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: 300 for the small grids, 30 for blobs256/gyroid320, 3 for batches)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="sdfgpu", choices=["sdfgpu", "reference"])
     ap.add_argument("--workload", default="torus128")
@@ -324,6 +330,8 @@ def main():
     ap.add_argument("--streams", type=int, default=8, help="batch workloads: worker streams")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.steps is None:
+        args.steps = 3 if args.workload.startswith("batch") else (30 if args.workload in ("blobs256", "gyroid320") else 300)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -454,6 +462,19 @@ def main():
     if os.path.exists(tpath):
         traffic = json.load(open(tpath)).get(args.workload, {}).get("k_tile_fold")
 
+    # FP32 roofline of the whole step (the path's bound is CUDA-core arithmetic, not tensor or HBM):
+    # the oracle's work model gives the algorithmic FP32 FLOPs per node, mean W (profiles/roofline.json,
+    # made by oracle/work_model.py); the peak is measured here on the same GPU.
+    roof32 = None
+    rpath = os.path.join(ROOT, "profiles", "roofline.json")
+    wm = json.load(open(rpath)).get(args.workload) if os.path.exists(rpath) else None
+    if wm:
+        p32 = _native.measure_fp32_peak(local)
+        bound = p32 * 1e12 / wm["mean_W_flop"]
+        roof32 = {"bound": "fp32", "mean_W_flop_per_node": wm["mean_W_flop"], "F_pt": wm["F_pt"], "F_mt": wm["F_mt"],
+                  "work_sample": wm["sample"], "peak": p32, "unit": "TFLOP/s", "peak_source": "measured (FMA probe)",
+                  "achieved": value * wm["mean_W_flop"] / 1e12, "roofline_nodes_per_s": bound, "frac": value / bound}
+
     line = {
         "metric": METRIC, "value": value, "unit": "nodes/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -467,6 +488,7 @@ def main():
         "roofline": {"bound": "hbm", "kernel": "k_tile_fold", "achieved": achieved, "peak": peak,
                      "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "alg_bytes_per_launch": int(alg_bytes), "ms_per_launch": fold_avg},
+        "roofline_fp32": roof32,
         "stages_ms": {k: stats[k] for k in ("ms_mesh", "ms_tiles", "ms_fold", "ms_rows", "ms_parity", "ms_vote",
                                              "ms_distance", "ms_sign")},
         "counters": {k: stats[k] for k in ("tile_pairs", "fp64_evals", "candidate_nodes", "row_hits",

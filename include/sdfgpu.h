@@ -259,6 +259,44 @@ int sdfgpu_radius_eval(sdfgpu_ctx* ctx, const float* xn, int64_t B, float* dhat)
 int sdfgpu_mlp_train_eval(sdfgpu_ctx* ctx, const float* params, const float* xn, const float* target, int64_t B,
                           float* dhat, float* loss, float* grad);
 
+/* remove_sdf_artifacts!(sdf, grid; threshold, min_component_ratio)
+ * (src/SignedDistances/SdfArtifactRemoval.jl:134-248), in place on the sdf of the grid with N cells
+ * per axis (ngp = prod(N+1) doubles, x fastest).  Interior nodes are sdf >= threshold; their
+ * 6-connected components smaller than max(1, round(min_component_ratio * largest)) (round to
+ * nearest, ties to even, as Julia's round(Int, x)), other than the largest, get sdf = -|sdf|.
+ * Writes the number of flipped nodes, of interior components and the size of the largest (any may
+ * be NULL).  Ties for the largest component go to the one with the smallest node index (they matter
+ * only for min_component_ratio > 1).  Needs no mesh.  sdf is host memory here and device memory of
+ * the context's device in the _device form (which runs on the context's stream and returns after
+ * it has finished). */
+int sdfgpu_remove_artifacts(sdfgpu_ctx* ctx, const int64_t N[3], double* sdf, double threshold,
+                            double min_component_ratio, int64_t* flipped, int64_t* components, int64_t* largest);
+int sdfgpu_remove_artifacts_device(sdfgpu_ctx* ctx, const int64_t N[3], double* d_sdf, double threshold,
+                                   double min_component_ratio, int64_t* flipped, int64_t* components,
+                                   int64_t* largest);
+/* analyze_sdf_components(sdf, grid; threshold) (SdfArtifactRemoval.jl:259-318): root_out (ngp
+ * int32, may be NULL) receives for every interior node the smallest linear index of its component
+ * (the component's label) and -1 for exterior nodes; also the component count and largest size. */
+int sdfgpu_sdf_components(sdfgpu_ctx* ctx, const int64_t N[3], const double* sdf, double threshold, int32_t* root_out,
+                          int64_t* components, int64_t* largest);
+
+/* RBFs_smoothing(dist, grid, is_interpolation, smooth, threshold) (src/SdfSmoothing/RBFs4Smoothing.jl:275-320):
+ * Gaussian RBFs of width cell_size, cut off where exp(-(r/cell_size)^2) <= threshold, centred on the
+ * nodes of the grid (aabb_min, aabb_max, N), with weights from conjugate gradients on K w = dist
+ * (interpolation = 1) or w = dist (interpolation = 0), evaluated on the grid refined `smooth` times
+ * per axis (fine_out: prod(N*smooth+1) floats, x fastest, Float32 like the reference's result).
+ * aabb_max is the grid's adjusted AABB_max (origin + N * cell_size).  weights_out (ngp floats),
+ * cg_iterations and cg_residual (final |r|) may be NULL.  CG stops as IterativeSolvers.cg does, at
+ * |r| <= sqrt(eps(Float32)) |dist|.  Needs no mesh. */
+int sdfgpu_rbf_smoothing(sdfgpu_ctx* ctx, const double aabb_min[3], const double aabb_max[3], const int64_t N[3],
+                         double cell_size, const double* dist, int32_t interpolation, int32_t smooth, double threshold,
+                         float* fine_out, float* weights_out, int32_t* cg_iterations, double* cg_residual);
+
+/* Measured FP32 CUDA-core throughput of `device` in TFLOP/s (independent FMA chains on every SM at
+ * full occupancy, best of five timed launches), the denominator of the hot path's FP32 roofline.
+ * No counterpart in the reference. */
+int sdfgpu_measure_fp32_peak(int32_t device, double* tflops);
+
 /* The cudaStream_t every kernel of the context runs on. */
 int sdfgpu_get_stream(sdfgpu_ctx* ctx, void** stream);
 int sdfgpu_get_stats(const sdfgpu_ctx* ctx, sdfgpu_stats* out);

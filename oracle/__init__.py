@@ -64,6 +64,8 @@ def lib():
         L.oracle_ray_triangle.argtypes = [_dp, _dp, _dp, _dp, _dp, ctypes.c_double, _dp]
         L.oracle_barycentric.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp]
         L.oracle_winding.argtypes = [_dp, ctypes.c_int64, _i64p, ctypes.c_int64, _dp, ctypes.c_int64, _dp, _dp, ctypes.c_int]
+        L.oracle_work_model.argtypes = [_dp, ctypes.c_int64, _i64p, ctypes.c_int64, _dp, ctypes.c_double, _i64p, _i64p,
+                                        ctypes.c_int64, _i64p, _i64p, _i64p, _i32p, ctypes.c_int]
         L.oracle_max_threads.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -173,6 +175,24 @@ def winding(X, IEN, pts, nthreads=0):
     if rc != 0:
         raise ValueError("oracle_winding failed")
     return s, w
+
+
+def work_model(X, IEN, origin, h, N, nodes, nthreads=0):
+    """Per-node algorithmic work counts: dict(nD, nrow (k x 3), nextra, rays); see oracle_work_model."""
+    X, IEN = _mesh_arrays(X, IEN)
+    N = np.asarray(N, dtype=np.int64)
+    origin = np.asarray(origin, dtype=np.float64)
+    nodes = np.ascontiguousarray(nodes, dtype=np.int64)
+    k = nodes.shape[0]
+    nD = np.empty(k, np.int64); nrow = np.empty((k, 3), np.int64); nextra = np.empty(k, np.int64)
+    rays = np.empty(k, np.int32)
+    rc = lib().oracle_work_model(_d(X), X.shape[0], IEN.ctypes.data_as(_i64p), IEN.shape[0], _d(origin), float(h),
+                                 N.ctypes.data_as(_i64p), nodes.ctypes.data_as(_i64p), k, nD.ctypes.data_as(_i64p),
+                                 nrow.ctypes.data_as(_i64p), nextra.ctypes.data_as(_i64p), rays.ctypes.data_as(_i32p),
+                                 int(nthreads))
+    if rc != 0:
+        raise ValueError("oracle_work_model failed")
+    return dict(nD=nD, nrow=nrow, nextra=nextra, rays=rays)
 
 
 def max_threads() -> int:

@@ -871,6 +871,98 @@ int oracle_winding(const double* X, int64_t nnp, const int64_t* IEN, int64_t nel
   return 0;
 }
 
+// Algorithmic work of the hot path at each listed node, independent of any implementation (the
+// roofline's work model):
+//   nD[q]      = |D*(p)|, triangles whose AABB lies within min(d_true(p), h) of p -- the
+//                candidates no box-pruned nearest search can skip (d_true: the unbounded minimum);
+//   nrow[3q+a] = triangles whose AABB meets the grid line through p along axis a (the +a and -a
+//                rays of every node of that row share them);
+//   nextra[q]  = triangles whose AABB the rays beyond the six axis rays hit (rays the reference's
+//                adaptive vote casts at p, RaycastingSignDetection.jl:234-288);
+//   rays[q]    = rays the vote casts at p.
+int oracle_work_model(const double* X, int64_t nnp, const int64_t* IEN, int64_t nel,
+                      const double origin[3], double h, const int64_t N[3], const int64_t* nodes,
+                      int64_t nnodes, int64_t* nD, int64_t* nrow, int64_t* nextra, int32_t* rays,
+                      int nthreads) {
+  if (nel <= 0 || nnp <= 0 || !nodes) return 1;
+  Grid g;
+  if (!grid_from(origin, h, N, g)) return 1;
+  Mesh M;
+  mesh_init(M, X, nnp, IEN, nel);
+  double D[36][3];
+  ray_directions(D);
+  const int nt = nthreads_for(nthreads);
+#pragma omp parallel num_threads(nt)
+  {
+    std::vector<int64_t> cand;
+    std::vector<double> ts;
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t q = 0; q < nnodes; ++q) {
+      const V3 p = node_coord(g, nodes[q]);
+      V3 proj;
+      int fl = 0;
+      const double dt = eval_node(M, g, p, MODE_UNBOUNDED, proj, fl, cand);
+      const double r = std::min(dt, g.h);
+      cand.clear();
+      query_ball(M.bvh, p, r, cand);
+      int64_t c = 0;
+      for (int64_t el : cand) {
+        const Tri& t = M.T[(size_t)el];
+        const double lo[3] = {t.bmin.x, t.bmin.y, t.bmin.z}, hi[3] = {t.bmax.x, t.bmax.y, t.bmax.z};
+        const double pc[3] = {p.x, p.y, p.z};
+        double s2 = 0.0;
+        for (int a = 0; a < 3; ++a) {
+          const double dd = pc[a] < lo[a] ? lo[a] - pc[a] : (pc[a] > hi[a] ? pc[a] - hi[a] : 0.0);
+          s2 += dd * dd;
+        }
+        if (s2 <= r * r) ++c;
+      }
+      nD[q] = c;
+      // grid lines: both coordinates other than a inside the triangle's box
+      const double pc[3] = {p.x, p.y, p.z};
+      for (int a = 0; a < 3; ++a) {
+        const int b = (a + 1) % 3, e = (a + 2) % 3;
+        int64_t cnt = 0;
+        int64_t st[128];
+        int sp = 0;
+        st[sp++] = 0;
+        while (sp) {
+          const BNode& nd = M.bvh.nodes[(size_t)st[--sp]];
+          if (pc[b] < nd.lo[b] || pc[b] > nd.hi[b] || pc[e] < nd.lo[e] || pc[e] > nd.hi[e]) continue;
+          if (nd.left < 0) {
+            for (int64_t i = nd.first; i < nd.first + nd.count; ++i) {
+              const Tri& t = M.T[(size_t)M.bvh.order[(size_t)i]];
+              const double lo[3] = {t.bmin.x, t.bmin.y, t.bmin.z}, hi[3] = {t.bmax.x, t.bmax.y, t.bmax.z};
+              if (pc[b] >= lo[b] && pc[b] <= hi[b] && pc[e] >= lo[e] && pc[e] <= hi[e]) ++cnt;
+            }
+          } else {
+            st[sp++] = nd.left;
+            st[sp++] = nd.right;
+          }
+        }
+        nrow[3 * q + a] = cnt;
+      }
+      double sg, cf, w;
+      int64_t nr;
+      int fb;
+      sign_node(M, p, D, 6, 30, 0.6, 1, sg, cf, &nr, &fb, &w, ts);
+      rays[q] = (int32_t)nr;
+      int64_t ex = 0;
+      for (int64_t rr = 6; rr < nr && rr < 36; ++rr) {
+        const V3 d{D[rr][0], D[rr][1], D[rr][2]};
+        for (const Tri& t : M.T) {
+          BNode bb{};
+          bb.lo[0] = t.bmin.x; bb.lo[1] = t.bmin.y; bb.lo[2] = t.bmin.z;
+          bb.hi[0] = t.bmax.x; bb.hi[1] = t.bmax.y; bb.hi[2] = t.bmax.z;
+          if (ray_box(bb, p, d)) ++ex;
+        }
+      }
+      nextra[q] = ex;
+    }
+  }
+  return 0;
+}
+
 int oracle_max_threads(void) { return nthreads_for(0); }
 
 }  // extern "C"

@@ -25,13 +25,15 @@ def exportSdfToVTI(filename: str, grid, values, value_label: str, smooth=None, c
     N = np.asarray(grid.N, dtype=np.int64)
     dims = N + 1 if smooth is None else N * int(smooth) + 1
     h = grid.cell_size if smooth is None else grid.cell_size / int(smooth)
-    values = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+    # WriteVTK writes the array's own element type: Float32 for the smoothed field, else Float64
+    vt = np.float32 if np.asarray(values).dtype == np.float32 else np.float64
+    values = np.ascontiguousarray(values, dtype=vt).reshape(-1)
     if values.shape[0] != int(np.prod(dims)):
         raise ValueError(f"Values vector length ({values.shape[0]}) doesn't match grid dimensions ({int(np.prod(dims))}).")
     o = [float(v) for v in np.asarray(grid.AABB_min, dtype=np.float64)]
     h = float(h)
     ext = f"0 {dims[0] - 1} 0 {dims[1] - 1} 0 {dims[2] - 1}"
-    raw = values.astype("<f8").tobytes()
+    raw = values.astype("<f4" if vt == np.float32 else "<f8").tobytes()
     if compress:
         comp = zlib.compress(raw, 6)
         payload = np.array([1, len(raw), len(raw), len(comp)], dtype="<u8").tobytes() + comp
@@ -46,7 +48,7 @@ def exportSdfToVTI(filename: str, grid, values, value_label: str, smooth=None, c
         'Direction="1 0 0 0 1 0 0 0 1">\n'
         f'    <Piece Extent="{ext}">\n'
         "      <PointData>\n"
-        f'        <DataArray type="Float64" Name="{value_label}" format="appended" offset="0"/>\n'
+        f'        <DataArray type="{"Float32" if vt == np.float32 else "Float64"}" Name="{value_label}" format="appended" offset="0"/>\n'
         "      </PointData>\n"
         "    </Piece>\n"
         "  </ImageData>\n"
@@ -81,7 +83,8 @@ def read_vti(path: str):
     else:
         n = int(np.frombuffer(blob[:8], dtype="<u8")[0])
         raw = blob[8:8 + n]
-    return np.frombuffer(raw, dtype="<f8").copy(), dims, origin, spacing, label
+    dt = "<f4" if 'type="Float32"' in head else "<f8"
+    return np.frombuffer(raw, dtype=dt).copy(), dims, origin, spacing, label
 
 
 def export_path(filename: str) -> str:

@@ -1,54 +1,41 @@
-"""Small-component removal, mirroring src/SignedDistances/SdfArtifactRemoval.jl:134-318.
+"""Small-component removal, mirroring src/SignedDistances/SdfArtifactRemoval.jl:134-318, on the GPU.
 
 Interior nodes are ``sdf >= threshold``; 6-connected interior components smaller than
 ``max(1, round(ratio * largest))`` (other than the largest) are flipped to ``-|sdf|``.  The
-reference labels components with a union-find inside ``@threads`` (racy, :164-182); component
-membership does not depend on the union order, so a deterministic labelling gives the
-reference's result.  Ties for the largest component do not matter: a tied component is at least
-the minimum size and is kept either way.
+labelling runs in libsdfgpu.so (``sdfgpu_remove_artifacts``, a lock-free union-find); the
+reference's threaded union-find (:164-182) is racy in its roots but not in its components, and
+the components are all the result depends on.  Component labels here are the smallest linear node
+index of each component (1-based in the returned dict, like the reference's linear indices).
 """
 
 from __future__ import annotations
 
 import numpy as np
 
-
-def _labels(mask3d: np.ndarray):
-    from scipy import ndimage
-
-    structure = ndimage.generate_binary_structure(3, 1)  # 6-connectivity
-    return ndimage.label(mask3d, structure=structure)
+from . import _native
 
 
-def analyze_sdf_components(sdf_values, grid, threshold: float = 0.0) -> dict:
+def analyze_sdf_components(sdf_values, grid, threshold: float = 0.0, device: int = 0) -> dict:
     """Component label -> size of the interior components (SdfArtifactRemoval.jl:259-318)."""
-    n = np.asarray(grid.N, dtype=np.int64) + 1
-    mask = (np.asarray(sdf_values) >= threshold).reshape(n[2], n[1], n[0])
-    lab, k = _labels(mask)
-    sizes = np.bincount(lab.reshape(-1), minlength=k + 1)[1:]
-    return {i + 1: int(s) for i, s in enumerate(sizes)}
+    ctx = _native.default_context(device)
+    roots, count, largest = ctx.components(np.asarray(grid.N, np.int64), np.asarray(sdf_values, np.float64),
+                                           threshold)
+    r = roots[roots >= 0]
+    labels, sizes = np.unique(r, return_counts=True)
+    return {int(a) + 1: int(b) for a, b in zip(labels, sizes)}
 
 
-def remove_sdf_artifacts(sdf_values: np.ndarray, grid, threshold: float = 0.0, min_component_ratio: float = 0.01) -> int:
+def remove_sdf_artifacts(sdf_values: np.ndarray, grid, threshold: float = 0.0, min_component_ratio: float = 0.01,
+                         device: int = 0) -> int:
     """In place: flip small interior components; returns the number of nodes flipped."""
     sdf = sdf_values
     if sdf.shape[0] != grid.ngp:
         raise ValueError(f"SDF values length ({sdf.shape[0]}) doesn't match grid points ({grid.ngp})")
-    n = np.asarray(grid.N, dtype=np.int64) + 1
-    mask = (sdf >= threshold).reshape(n[2], n[1], n[0])
-    if not mask.any():
-        return 0
-    lab, k = _labels(mask)
-    sizes = np.bincount(lab.reshape(-1), minlength=k + 1)
-    sizes[0] = 0
-    largest = int(np.argmax(sizes))
-    min_size = max(1, int(round(min_component_ratio * sizes[largest])))
-    small = sizes < min_size
-    small[0] = False
-    small[largest] = False
-    flip = small[lab.reshape(-1)]
-    sdf[flip] = -np.abs(sdf[flip])
-    return int(np.count_nonzero(flip))
+    if sdf.dtype != np.float64 or not sdf.flags.c_contiguous:
+        raise TypeError("sdf_values must be a contiguous float64 vector")
+    ctx = _native.default_context(device)
+    flipped, _, _ = ctx.remove_artifacts(np.asarray(grid.N, np.int64), sdf, threshold, min_component_ratio)
+    return flipped
 
 
 remove_sdf_artifacts_ = remove_sdf_artifacts

@@ -13,12 +13,13 @@ import os
 
 import numpy as np
 
-from . import DataExport, DataImport, MeshGrid, SignedDistances
+from . import DataExport, DataImport, MeshGrid, SdfSmoothing, SignedDistances
 from .DataExport import exportSdfToVTI
 from .DataImport import import_stl
 from .MeshGrid import (Grid, TriangularMesh, generateGridPoints, getMesh_AABB, interactive_sdf_grid_setup,
                        noninteractive_sdf_grid_setup)
 from .SdfArtifactRemoval import analyze_sdf_components, remove_sdf_artifacts
+from .SdfSmoothing import RBFs_smoothing
 from .SignedDistances import evalDistancesOnTriMesh, raycast_sign_detection, signed_distance_field
 from ._native import SdfGpuError
 
@@ -26,7 +27,7 @@ __all__ = [
     "Options", "stl_to_sdf", "import_stl", "TriangularMesh", "Grid", "generateGridPoints", "getMesh_AABB",
     "noninteractive_sdf_grid_setup", "interactive_sdf_grid_setup", "evalDistancesOnTriMesh",
     "raycast_sign_detection", "signed_distance_field", "remove_sdf_artifacts", "analyze_sdf_components",
-    "exportSdfToVTI", "SdfGpuError",
+    "exportSdfToVTI", "RBFs_smoothing", "SdfGpuError",
 ]
 
 
@@ -46,7 +47,8 @@ class Options:
 def stl_to_sdf(stl_filename: str, options: Options = None, out_dir: str = "."):
     """stl_to_sdf (src/stl_to_sdf.jl:75-147): STL -> mesh -> grid -> distances x signs -> VTI.
 
-    Writes ``<base>_sdf.vti`` (point field "distance") into out_dir and returns
+    Writes ``<base>_sdf.vti`` (point field "distance") into out_dir, and with a smoothing method
+    also ``<base>_fine_sdf.vti`` (the RBF-smoothed field on the refined grid, Float32).  Returns
     (sdf, grid, path).
     """
     options = options or Options()
@@ -56,8 +58,6 @@ def stl_to_sdf(stl_filename: str, options: Options = None, out_dir: str = "."):
         raise AssertionError("grid_refinement must be 1 or 2")
     if not (0.0 < options.artifact_ratio < 1.0):
         raise AssertionError("artifact_ratio must be in range (0, 1)")
-    if options.smoothing_method is not None:
-        raise NotImplementedError("RBF smoothing (RBFs_smoothing) is not part of this build")
     base = os.path.splitext(os.path.basename(stl_filename))[0]
     X, IEN = import_stl(stl_filename)
     mesh = TriangularMesh(X, IEN)
@@ -73,4 +73,8 @@ def stl_to_sdf(stl_filename: str, options: Options = None, out_dir: str = "."):
         flipped = remove_sdf_artifacts(sdf, grid, min_component_ratio=options.artifact_ratio)
         print(f"Artifact removal completed: {flipped} nodes modified")
     path = exportSdfToVTI(os.path.join(out_dir, f"{base}_sdf.vti"), grid, sdf, "distance")
+    if options.smoothing_method is not None:
+        fine_sdf, fine_grid = RBFs_smoothing(sdf, grid, options.smoothing_method == "interpolation",
+                                             options.grid_refinement)
+        exportSdfToVTI(os.path.join(out_dir, f"{base}_fine_sdf.vti"), fine_grid, fine_sdf, "distance")
     return sdf, grid, path

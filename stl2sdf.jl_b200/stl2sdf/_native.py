@@ -108,6 +108,16 @@ SIGNATURES = {
                          ctypes.POINTER(ctypes.c_int32), _dp], ctypes.c_int),
     "sdfgpu_set_brick": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
     "sdfgpu_set_radius_margin": ([ctypes.c_void_p, ctypes.c_float, ctypes.c_float], ctypes.c_int),
+    "sdfgpu_measure_fp32_peak": ([ctypes.c_int32, _dp], ctypes.c_int),
+    "sdfgpu_remove_artifacts": ([ctypes.c_void_p, _i64p, _dp, ctypes.c_double, ctypes.c_double, _i64p, _i64p, _i64p],
+                                ctypes.c_int),
+    "sdfgpu_remove_artifacts_device": ([ctypes.c_void_p, _i64p, ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                                        _i64p, _i64p, _i64p], ctypes.c_int),
+    "sdfgpu_rbf_smoothing": ([ctypes.c_void_p, _dp, _dp, _i64p, ctypes.c_double, _dp, ctypes.c_int32, ctypes.c_int32,
+                              ctypes.c_double, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                              ctypes.POINTER(ctypes.c_int32), _dp], ctypes.c_int),
+    "sdfgpu_sdf_components": ([ctypes.c_void_p, _i64p, _dp, ctypes.c_double, ctypes.POINTER(ctypes.c_int32), _i64p,
+                               _i64p], ctypes.c_int),
     "sdfgpu_get_stream": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "sdfgpu_get_stats": ([ctypes.c_void_p, ctypes.POINTER(Stats)], ctypes.c_int),
 }
@@ -351,10 +361,64 @@ class Context:
                                                 grad.ctypes.data_as(fp)))
         return dh, float(loss[0]), grad
 
+    # ---- artifact removal (SdfArtifactRemoval.jl) ----
+    def remove_artifacts(self, N, sdf, threshold=0.0, min_component_ratio=0.01):
+        """In place on the float64 array sdf; returns (flipped, components, largest)."""
+        N = np.ascontiguousarray(N, np.int64)
+        if sdf.dtype != np.float64 or not sdf.flags.c_contiguous or sdf.size != int(np.prod(N + 1)):
+            raise ValueError("sdf must be a contiguous float64 array of prod(N+1) values")
+        f, c, l = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        self._check(lib().sdfgpu_remove_artifacts(self._p, _i(N), sdf.ctypes.data_as(_dp), float(threshold),
+                                                  float(min_component_ratio), ctypes.byref(f), ctypes.byref(c),
+                                                  ctypes.byref(l)))
+        return f.value, c.value, l.value
+
+    def components(self, N, sdf, threshold=0.0):
+        """Per node the smallest linear index of its interior component (-1 exterior), count, largest."""
+        N = np.ascontiguousarray(N, np.int64)
+        sdf = np.ascontiguousarray(sdf, np.float64)
+        if sdf.size != int(np.prod(N + 1)):
+            raise ValueError("sdf must hold prod(N+1) values")
+        roots = np.empty(sdf.size, np.int32)
+        c, l = ctypes.c_int64(), ctypes.c_int64()
+        self._check(lib().sdfgpu_sdf_components(self._p, _i(N), sdf.ctypes.data_as(_dp), float(threshold),
+                                                roots.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(c),
+                                                ctypes.byref(l)))
+        return roots, c.value, l.value
+
+    # ---- RBF smoothing (RBFs4Smoothing.jl) ----
+    def rbf_smoothing(self, aabb_min, aabb_max, N, cell_size, dist, interpolation=True, smooth=2, threshold=1e-3,
+                      want_weights=False):
+        """Returns (fine Float32 values, x fastest; weights or None; CG iterations; final |r|)."""
+        N = np.ascontiguousarray(N, np.int64)
+        lo = np.ascontiguousarray(aabb_min, np.float64)
+        hi = np.ascontiguousarray(aabb_max, np.float64)
+        dist = np.ascontiguousarray(dist, np.float64)
+        if dist.size != int(np.prod(N + 1)):
+            raise ValueError("dist must hold prod(N+1) values")
+        fine = np.empty(int(np.prod(N * int(smooth) + 1)), np.float32)
+        w = np.empty(dist.size, np.float32) if want_weights else None
+        fp = ctypes.POINTER(ctypes.c_float)
+        it, res = ctypes.c_int32(), ctypes.c_double()
+        self._check(lib().sdfgpu_rbf_smoothing(self._p, _d(lo), _d(hi), _i(N), float(cell_size), _d(dist),
+                                               int(bool(interpolation)), int(smooth), float(threshold),
+                                               fine.ctypes.data_as(fp), w.ctypes.data_as(fp) if w is not None else None,
+                                               ctypes.byref(it), ctypes.byref(res)))
+        return fine, w, it.value, res.value
+
     def stats(self) -> dict:
         s = Stats()
         self._check(lib().sdfgpu_get_stats(self._p, ctypes.byref(s)))
         return s.as_dict()
+
+
+def measure_fp32_peak(device: int = 0) -> float:
+    """Measured FP32 CUDA-core throughput of the device (TFLOP/s)."""
+    t = ctypes.c_double(0.0)
+    rc = lib().sdfgpu_measure_fp32_peak(int(device), ctypes.byref(t))
+    if rc:
+        raise SdfGpuError(rc, "sdfgpu_measure_fp32_peak failed")
+    return t.value
 
 
 _default_ctx = {}

@@ -308,3 +308,11 @@ def test_unbounded_brick_autotune(gpu_ctx, icosphere_mesh):
     d1, _ = gpu_ctx.distances(g["origin"], g["h"], g["N"], 2)
     gpu_ctx.set_brick((4, 2, 4))
     assert np.array_equal(d0, d1)
+
+
+def test_fp32_peak_probe():
+    from stl2sdf import _native
+
+    t = _native.measure_fp32_peak(0)
+    # 148 SMs x 128 FP32 lanes x 2 FLOPs at 1.0-2.0 GHz: well inside (20, 100) TFLOP/s
+    assert 20.0 < t < 100.0, t

@@ -105,19 +105,41 @@ def test_grid_points_match_oracle_nodes(icosphere_mesh):
     assert len(mesh.INE) == mesh.nnp and sum(len(v) for v in mesh.INE) == 3 * mesh.nel
 
 
-def test_artifact_removal():
-    from stl2sdf import MeshGrid, remove_sdf_artifacts, analyze_sdf_components
-
-    g = MeshGrid.Grid.from_parts([0.0, 0.0, 0.0], [19, 19, 19], 0.1)
-    n = g.N + 1
-    sdf = -np.ones(g.ngp)
+def _two_blobs():
+    N = np.array([19, 19, 19])
+    n = N + 1
+    sdf = -np.ones(int(np.prod(n)))
     vol = sdf.reshape(n[2], n[1], n[0])
     vol[2:12, 2:12, 2:12] = 1.0   # large interior component (1000 nodes)
     vol[15:17, 15:17, 15:16] = 1.0  # small one (4 nodes)
-    comps = analyze_sdf_components(sdf, g)
-    assert sorted(comps.values()) == [4, 1000]
-    flipped = remove_sdf_artifacts(sdf, g, min_component_ratio=0.01)
-    assert flipped == 4 and np.count_nonzero(sdf > 0) == 1000
+    return N, sdf
+
+
+def test_artifact_removal_oracle_known_answer():
+    from oracle import artifacts
+
+    N, sdf = _two_blobs()
+    out, flipped, comps, largest = artifacts.remove_sdf_artifacts(sdf, N, min_component_ratio=0.01)
+    assert (flipped, comps, largest) == (4, 2, 1000)
+    assert np.count_nonzero(out > 0) == 1000 and np.count_nonzero(sdf > 0) == 1004
+    # ratio 0.004 -> min size round(4.0) = 4: the 4-node component stays
+    _, flipped, _, _ = artifacts.remove_sdf_artifacts(sdf, N, min_component_ratio=0.004)
+    assert flipped == 0
+    # round half to even, as Julia's round(Int, x): 0.0045 * 1000 = 4.5 -> 4, the 4-node component stays
+    _, flipped, _, _ = artifacts.remove_sdf_artifacts(sdf, N, min_component_ratio=0.0045)
+    assert flipped == 0
+    _, flipped, _, _ = artifacts.remove_sdf_artifacts(sdf, N, min_component_ratio=0.0055)
+    assert flipped == 4
+
+
+def test_artifact_labelling_matches_union_find():
+    from oracle import artifacts
+
+    rng = np.random.default_rng(5)
+    for shape in ([6, 5, 4], [9, 1, 7], [0, 0, 0], [3, 3, 3]):
+        n = np.asarray(shape) + 1
+        mask = rng.random(int(np.prod(n))) < 0.45
+        assert np.array_equal(artifacts.labels(mask, n), artifacts.union_find_labels(mask, n))
 
 
 def test_options_validation():
