@@ -288,6 +288,8 @@ def run_batch(args, rank, world, local):
         "single_stream_default_tile": {"value": total / one, "s": one},
         "first_call_s": t_tune,
         "stages_ms_summed": {k: st[k] for k in ("ms_mesh", "ms_tiles", "ms_fold", "ms_rows", "ms_parity", "ms_vote")},
+        "counters_summed": {k: st[k] for k in ("tile_pairs", "fp64_evals", "row_hits", "undecided_nodes", "extra_rays",
+                                                "winding_nodes", "knn_fallback_nodes", "launches", "mesh_launches")},
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -474,12 +474,15 @@ __device__ __noinline__ void step64_call(const TriRec64* rec, int prim, const d3
 // Per-lane state of the FP32 search: the smallest FP32 point-triangle distance m (INF before the
 // first hit) and the triangles whose FP32 distance lies within band(m) = m + 2 err(m), one of
 // which is the true (FP64) nearest: |FP32 - FP64| <= err for every distance, so the FP64 winner t*
-// has D32(t*) <= d64(t*) + err <= d64(t_m) + err <= m + 2 err.  Slots hold INF when free.
+// has D32(t*) <= d64(t*) + err <= d64(t_m) + err <= m + 2 err.  The kept triangles live in shared
+// memory (slot q of thread x at q * kUnbThreads + x: consecutive threads, consecutive banks), which
+// keeps the traversal's registers low enough for three CTAs per SM.  Free slots hold INF.
+constexpr int kUnbThreads = kUnbWarps * 32;
 struct LaneBest {
   float m;
   bool overflow;  // the band held more than kKeep triangles at some point
-  int t[kKeep];
-  float d[kKeep];
+  int* t;         // shared: kept triangle ids
+  float* d;       // shared: their FP32 distances
 };
 
 __device__ __forceinline__ float band_of(const UnbArgs& A, float m) { return m + 2.f * (A.eD_abs + A.eD_rel * m); }
@@ -490,22 +493,25 @@ __device__ __forceinline__ void lane_offer(const UnbArgs& A, LaneBest& L, float 
     const float bd = band_of(A, D);
 #pragma unroll
     for (int q = 0; q < kKeep; ++q)
-      if (L.d[q] > bd) L.d[q] = INFINITY;
+      if (L.d[q * kUnbThreads] > bd) L.d[q * kUnbThreads] = INFINITY;
   } else if (D > band_of(A, L.m)) {
     return;
   }
-  bool placed = false;
+  int free_q = -1;
+  bool dup = false;
 #pragma unroll
-  for (int q = 0; q < kKeep; ++q)
-    if (L.d[q] != INFINITY && L.t[q] == tri) placed = true;  // already kept (a second pass)
-#pragma unroll
-  for (int q = 0; q < kKeep; ++q)
-    if (!placed && L.d[q] == INFINITY) {
-      L.d[q] = D;
-      L.t[q] = tri;
-      placed = true;
-    }
-  if (!placed) L.overflow = true;
+  for (int q = 0; q < kKeep; ++q) {
+    const float dq = L.d[q * kUnbThreads];
+    if (dq != INFINITY && L.t[q * kUnbThreads] == tri) dup = true;  // already kept (a second pass)
+    if (free_q < 0 && dq == INFINITY) free_q = q;
+  }
+  if (dup) return;
+  if (free_q < 0) {
+    L.overflow = true;
+    return;
+  }
+  L.d[free_q * kUnbThreads] = D;
+  L.t[free_q * kUnbThreads] = tri;
 }
 
 // One warp searches the LBVH for the nearest triangles of its 32 nodes together (a packet
@@ -598,8 +604,10 @@ __device__ __forceinline__ void lane_resolve(const UnbArgs& A, const LaneBest& L
   for (int it = 0; it < kKeep; ++it) {
     int best = 0x7fffffff;
 #pragma unroll
-    for (int q = 0; q < kKeep; ++q)
-      if (L.d[q] <= bd && L.t[q] > last && L.t[q] < best) best = L.t[q];
+    for (int q = 0; q < kKeep; ++q) {
+      const int tq = L.t[q * kUnbThreads];
+      if (L.d[q * kUnbThreads] <= bd && tq > last && tq < best) best = tq;
+    }
     if (best == 0x7fffffff) break;
     step64_call(A.rec, best, p, m64, proj);
     ++fp64;
@@ -612,8 +620,10 @@ __device__ __forceinline__ void lane_resolve(const UnbArgs& A, const LaneBest& L
 // nearer triangle lies within r and was visited), and the lanes without one search again without
 // the bound, keeping what they found.  Lanes whose band overflowed search once more with FP64
 // steps bounded by the band.
-__global__ void __launch_bounds__(kUnbWarps * 32, 2) k_unbounded(UnbArgs A) {
+__global__ void __launch_bounds__(kUnbThreads, 3) k_unbounded(UnbArgs A) {
   __shared__ int s_stack[kUnbWarps][kWarpStack];
+  __shared__ int s_keep_t[kKeep * kUnbThreads];
+  __shared__ float s_keep_d[kKeep * kUnbThreads];
   const GridP& g = A.g;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int* stack = s_stack[w];
@@ -632,10 +642,12 @@ __global__ void __launch_bounds__(kUnbWarps * 32, 2) k_unbounded(UnbArgs A) {
     LaneBest L;
     L.m = INFINITY;
     L.overflow = false;
+    L.t = s_keep_t + threadIdx.x;
+    L.d = s_keep_d + threadIdx.x;
 #pragma unroll
     for (int q = 0; q < kKeep; ++q) {
-      L.t[q] = -1;
-      L.d[q] = INFINITY;
+      L.t[q * kUnbThreads] = -1;
+      L.d[q * kUnbThreads] = INFINITY;
     }
     double m64 = kBig;
     d3 proj = {0.0, 0.0, 0.0};

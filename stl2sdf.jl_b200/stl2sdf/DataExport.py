@@ -3,8 +3,9 @@
 The file holds one point field (``value_label``) over an ImageData with extent 0..N per axis,
 origin ``grid.AABB_min`` and spacing ``cell_size`` (``cell_size/smooth`` with ``N*smooth`` cells
 when ``smooth`` is given), values in the grid's x-fastest order.  The layout is the one WriteVTK
-writes for ``vtk_grid(filename, x, y, z)``: appended raw binary, UInt64 block headers, and (by
-default, like WriteVTK) a single zlib-compressed block.
+writes for ``vtk_grid(filename, x, y, z)``: appended raw binary, UInt64 block headers and zlib
+compression (one block up to 4 MiB, as WriteVTK; larger fields in 4 MiB blocks compressed in
+parallel).
 """
 
 from __future__ import annotations
@@ -14,6 +15,27 @@ import re
 import zlib
 
 import numpy as np
+
+
+_BLOCK = 1 << 22  # 4 MiB uncompressed per zlib block
+
+
+def _zlib_blocks(raw: bytes) -> bytes:
+    """vtkZLibDataCompressor payload: UInt64 header [nblocks, block size, last block size,
+    compressed sizes...] and the zlib streams of the blocks.  A field of one block is what WriteVTK
+    writes; larger fields are cut into 4 MiB blocks compressed on all host cores (zlib releases the
+    GIL), which every VTK reader accepts."""
+    blocks = [raw[i:i + _BLOCK] for i in range(0, len(raw), _BLOCK)] or [b""]
+    if len(blocks) == 1:
+        comp = [zlib.compress(blocks[0], 6)]
+    else:
+        from concurrent.futures import ThreadPoolExecutor
+
+        with ThreadPoolExecutor(max_workers=min(len(blocks), os.cpu_count() or 1)) as ex:
+            comp = list(ex.map(lambda b: zlib.compress(b, 6), blocks))
+    last = len(blocks[-1])
+    hdr = np.array([len(blocks), len(blocks[0]) if len(blocks) > 1 else last, last] + [len(c) for c in comp], dtype="<u8")
+    return hdr.tobytes() + b"".join(comp)
 
 
 def _vti_name(filename: str) -> str:
@@ -35,8 +57,7 @@ def exportSdfToVTI(filename: str, grid, values, value_label: str, smooth=None, c
     ext = f"0 {dims[0] - 1} 0 {dims[1] - 1} 0 {dims[2] - 1}"
     raw = values.astype("<f4" if vt == np.float32 else "<f8").tobytes()
     if compress:
-        comp = zlib.compress(raw, 6)
-        payload = np.array([1, len(raw), len(raw), len(comp)], dtype="<u8").tobytes() + comp
+        payload = _zlib_blocks(raw)
         comp_attr = ' compressor="vtkZLibDataCompressor"'
     else:
         payload = np.array([len(raw)], dtype="<u8").tobytes() + raw
@@ -77,9 +98,13 @@ def read_vti(path: str):
     label = re.search(r'Name="([^"]+)"', head).group(1)
     blob = body[us:]
     if "vtkZLibDataCompressor" in head:
-        hdr = np.frombuffer(blob[:32], dtype="<u8")
-        clen = int(hdr[3])
-        raw = zlib.decompress(blob[32:32 + clen])
+        nb = int(np.frombuffer(blob[:8], dtype="<u8")[0])
+        hdr = np.frombuffer(blob[:8 * (3 + nb)], dtype="<u8")
+        pos, parts = 8 * (3 + nb), []
+        for c in hdr[3:]:
+            parts.append(zlib.decompress(blob[pos:pos + int(c)]))
+            pos += int(c)
+        raw = b"".join(parts)
     else:
         n = int(np.frombuffer(blob[:8], dtype="<u8")[0])
         raw = blob[8:8 + n]

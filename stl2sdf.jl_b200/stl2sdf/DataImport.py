@@ -33,9 +33,16 @@ def detect_stl_type(filename: str) -> bool:
 def read_binary_stl(filename: str):
     """Raw (non-deduplicated) float64 vertices, 3 per triangle, and 1-based triangles."""
     with open(filename, "rb") as f:
-        f.seek(80)
-        n = int(np.frombuffer(f.read(4), dtype="<u4")[0])
-        rec = np.frombuffer(f.read(n * 50), dtype=_STL_DTYPE, count=n)
+        head = f.read(84)
+        if len(head) < 84:
+            raise ValueError(f"{filename}: not a binary STL (shorter than its 84-byte header)")
+        n = int(np.frombuffer(head[80:84], dtype="<u4")[0])
+        body = f.read(n * 50)
+    if len(body) < n * 50:
+        # the reference's read loop hits end-of-file here (ImportStlData.jl:136-156)
+        raise ValueError(f"{filename}: truncated binary STL: the header announces {n} triangles, "
+                         f"the file holds {len(body) // 50}")
+    rec = np.frombuffer(body, dtype=_STL_DTYPE, count=n)
     V = rec["v"].reshape(-1, 3).astype(np.float64)
     T = np.arange(1, 3 * n + 1, dtype=np.int64).reshape(n, 3)
     return V, T

@@ -215,6 +215,16 @@ def test_errors_are_reported(gpu_ctx):
         ctx.distances([0, 0, 0], -1.0, [3, 3, 3])
     with pytest.raises(_native.SdfGpuError):
         ctx.signs([0, 0, 0], 0.1, [3, 3, 3], min_rays=0)
+    # a grid beyond 2^31 - 1 nodes is refused before anything is allocated (z slabs split it)
+    with pytest.raises(_native.SdfGpuError, match="2\\^31") as e:
+        ctx.distances([0, 0, 0], 0.1, [2000, 2000, 2000])
+    assert e.value.code == 1
+    # non-finite vertices are rejected by the mesh upload
+    Xn = np.eye(3)
+    Xn[1, 2] = np.nan
+    with pytest.raises(_native.SdfGpuError, match="finite") as e:
+        ctx.set_mesh(Xn, np.array([[1, 2, 3]]))
+    assert e.value.code == 1
     ctx.close()
 
 
@@ -264,6 +274,28 @@ def test_blobs_full_size_sample(gpu_ctx):
     assert np.all((dist >= 0) & (dist <= g["h"]))
     assert np.all(np.abs(sign) == 1.0) and np.array_equal(sdf, dist * sign)
     nodes = sample_nodes(g["ngp"], 3000, seed=11)
+    dr, _, _ = oracle.distances(X, IEN, g["origin"], g["h"], g["N"], mode=0, nodes=nodes)
+    check_dist(dist[nodes], dr, X)
+    ref = oracle.signs(X, IEN, g["origin"], g["h"], g["N"], nodes=nodes)
+    assert np.array_equal(sign[nodes], ref["sign"]) and np.array_equal(conf[nodes], ref["conf"])
+
+
+def test_gyroid_full_size_sample(gpu_ctx):
+    """Workload 5 mesh (gyroid sheet at 384^3, ~5.7M triangles) on its 320-node grid: every node on
+    the GPU; in the oracle 1,500 seeded uniform nodes plus 1,500 seeded nodes within one cell of the
+    sheet (where grazing axis rays, edge/vertex hits and near-equidistant triangles are)."""
+    from stl2sdf import DataImport, synthetic
+
+    V, F = synthetic.gyroid(384, 0.04, 2.0)
+    X, IEN = DataImport.roundtrip_float32(V, F)
+    g = grid_of(X, n_nodes_long_axis=320)
+    gpu_ctx.set_mesh(X, IEN)
+    sdf, dist, sign, conf = gpu_ctx.sdf(g["origin"], g["h"], g["N"], want_parts=True)
+    assert np.array_equal(sdf, dist * sign)
+    rng = np.random.default_rng(17)
+    near = np.flatnonzero(dist < g["h"])
+    nodes = np.unique(np.concatenate([sample_nodes(g["ngp"], 1500, seed=17),
+                                      rng.choice(near, size=min(1500, near.size), replace=False)])).astype(np.int64)
     dr, _, _ = oracle.distances(X, IEN, g["origin"], g["h"], g["N"], mode=0, nodes=nodes)
     check_dist(dist[nodes], dr, X)
     ref = oracle.signs(X, IEN, g["origin"], g["h"], g["N"], nodes=nodes)

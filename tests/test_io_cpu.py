@@ -142,6 +142,29 @@ def test_artifact_labelling_matches_union_find():
         assert np.array_equal(artifacts.labels(mask, n), artifacts.union_find_labels(mask, n))
 
 
+def test_malformed_stl_is_reported(tmp_path):
+    from stl2sdf import DataImport, synthetic
+
+    V, F = synthetic.icosphere(1)
+    good = tmp_path / "good.stl"
+    DataImport.write_binary_stl(str(good), V, F)
+    data = good.read_bytes()
+    short = tmp_path / "short.stl"
+    short.write_bytes(data[:84 + 50 * 3 + 7])
+    with pytest.raises(ValueError, match="truncated binary STL"):
+        DataImport.import_stl(str(short))
+    tiny = tmp_path / "tiny.stl"
+    tiny.write_bytes(b"\x00" * 40)
+    with pytest.raises(ValueError, match="84-byte header"):
+        DataImport.import_stl(str(tiny))
+    nan = tmp_path / "nan.stl"
+    arr = bytearray(data)
+    arr[84 + 12:84 + 16] = np.float32(np.nan).tobytes()
+    nan.write_bytes(bytes(arr))
+    with pytest.raises(ValueError, match="finite"):
+        DataImport.import_stl(str(nan))
+
+
 def test_options_validation():
     import stl2sdf
 
