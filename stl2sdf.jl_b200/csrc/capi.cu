@@ -237,13 +237,29 @@ int run_all(sdfgpu_ctx* ctx, const GridP& g, bool want_dist, bool want_sign, int
   SDF_TRY(reset_counters(ctx));
   ctx->launches = 0;
   for (int i = 0; i < T_NUM; ++i) SDF_MARK(ctx, i);
+  // The sign stage runs on its own stream, forked after the counters are cleared: its row counting
+  // is enqueued first, the distance stage next (its one host wait covers the row count too), and
+  // the rest of the sign stage while the distance fold runs.  The join precedes the combine.
+  cudaStream_t ss = ctx->sign_stream;
+  SignPlan P;
+  if (want_sign) {
+    SDF_CUDA(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
+    SDF_CUDA(ctx, cudaStreamWaitEvent(ss, ctx->ev_fork, 0));
+    SDF_MARK_ON(ctx, T_SIGN0, ss);
+    SDF_TRY(sign_begin(ctx, g, P));
+  }
   if (want_dist) SDF_TRY(run_distances(ctx, g, mode, learned, d_dist, d_xp));
   SDF_MARK(ctx, T_DIST1);
-  for (int i = T_ROWS; i < T_NUM; ++i) SDF_MARK(ctx, i);
-  // Rays past the 36th are never cast, so every max_rays >= 44 gives the same votes as 44.
-  const int max_eff = max_rays > 44 ? 44 : max_rays;
-  if (want_sign) SDF_TRY(run_signs(ctx, g, min_rays, max_eff, conf, use_winding, d_dist, d_sign, d_conf, d_sdf));
-  SDF_MARK(ctx, T_SIGN1);
+  if (want_sign) {
+    for (int i = T_ROWS; i <= T_PARITY; ++i) SDF_MARK_ON(ctx, i, ss);
+    // Rays past the 36th are never cast, so every max_rays >= 44 gives the same votes as 44.
+    const int max_eff = max_rays > 44 ? 44 : max_rays;
+    SDF_TRY(sign_finish(ctx, g, P, min_rays, max_eff, conf, use_winding, d_sign, d_conf));
+    SDF_MARK_ON(ctx, T_SIGN1, ss);
+    SDF_CUDA(ctx, cudaEventRecord(ctx->ev_join, ss));
+    SDF_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+  }
+  if (want_dist && want_sign && d_sdf) SDF_TRY(run_combine(ctx, g, d_dist, d_sign, d_sdf));
   SDF_TRY(finish_counters(ctx, g));
   auto span = [&](int a, int b, double* out) -> int {
     float ms = 0.f;
@@ -253,10 +269,10 @@ int run_all(sdfgpu_ctx* ctx, const GridP& g, bool want_dist, bool want_sign, int
   };
   sdfgpu_stats& s = ctx->stats;
   SDF_TRY(span(T_DIST0, T_DIST1, &s.ms_distance));
-  SDF_TRY(span(T_DIST1, T_SIGN1, &s.ms_sign));
+  SDF_TRY(span(T_SIGN0, T_SIGN1, &s.ms_sign));
   SDF_TRY(span(T_DIST0, T_TILES, &s.ms_tiles));
   SDF_TRY(span(T_TILES, T_FOLD, &s.ms_fold));
-  SDF_TRY(span(T_DIST1, T_ROWS, &s.ms_rows));
+  SDF_TRY(span(T_SIGN0, T_ROWS, &s.ms_rows));
   SDF_TRY(span(T_ROWS, T_PARITY, &s.ms_parity));
   SDF_TRY(span(T_PARITY, T_SIGN1, &s.ms_vote));
   if (!want_dist) s.ms_distance = s.ms_tiles = s.ms_fold = 0.0;
@@ -355,6 +371,12 @@ int sdfgpu_create(const sdfgpu_opts* opts, sdfgpu_ctx** out) {
   };
   if ((e = cudaSetDevice(dev)) != cudaSuccess) return bail("cudaSetDevice", e);
   if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail("cudaStreamCreate", e);
+  if ((e = cudaStreamCreateWithFlags(&ctx->sign_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return bail("cudaStreamCreate", e);
+  for (cudaEvent_t* ev : {&ctx->ev_fork, &ctx->ev_join, &ctx->ev_rows})
+    if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return bail("cudaEventCreate", e);
+  if ((e = cudaHostAlloc((void**)&ctx->h_scalars, sizeof(int64_t) * S_NUM, cudaHostAllocDefault)) != cudaSuccess)
+    return bail("cudaHostAlloc", e);
   for (auto& ev : ctx->ev)
     if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail("cudaEventCreate", e);
   for (auto& ev : ctx->tev)
@@ -377,6 +399,7 @@ int sdfgpu_destroy(sdfgpu_ctx* ctx) {
   for (sdfgpu_ctx* w : ctx->workers) sdfgpu_destroy(w);
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->sign_stream) cudaStreamSynchronize(ctx->sign_stream);
   for (auto& kv : ctx->bufs)
     if (kv.second.p) cudaFree(kv.second.p);
   if (ctx->d_counters) cudaFree(ctx->d_counters);
@@ -384,6 +407,10 @@ int sdfgpu_destroy(sdfgpu_ctx* ctx) {
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : ctx->tev)
     if (ev) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : {ctx->ev_fork, ctx->ev_join, ctx->ev_rows})
+    if (ev) cudaEventDestroy(ev);
+  if (ctx->h_scalars) cudaFreeHost(ctx->h_scalars);
+  if (ctx->sign_stream) cudaStreamDestroy(ctx->sign_stream);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return SDFGPU_OK;

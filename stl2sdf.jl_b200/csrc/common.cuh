@@ -107,6 +107,9 @@ struct sdfgpu_ctx {
   sdfgpu::RadiusNorm radius;  // learned search radius (radius.cu)
   int64_t launches = 0;  // kernels of this library launched since the last reset
   cudaEvent_t tev[8] = {};  // stage timestamps, see sdfgpu::Stage
+  cudaStream_t sign_stream = nullptr;    // the sign stage runs here, beside the distance stage
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_rows = nullptr;
+  int64_t* h_scalars = nullptr;          // page-locked host slots for sizing reads (see Scalar)
   std::vector<sdfgpu_ctx*> workers;      // batch workers (batch.cu), created on first use
   std::map<int64_t, uint32_t> tuned;     // autotuner: size class -> packed tile (batch.cu)
 };
@@ -132,9 +135,14 @@ int fail(sdfgpu_ctx* ctx, int code, const std::string& msg);
     ++(ctx)->launches;                          \
   } while (0)
 
-// Stage timestamps recorded on the context stream.
-enum Stage : int { T_DIST0 = 0, T_TILES, T_FOLD, T_DIST1, T_ROWS, T_PARITY, T_SIGN1, T_NUM };
+// Stage timestamps: the distance stage's on the context stream, the sign stage's on its stream.
+enum Stage : int { T_DIST0 = 0, T_TILES, T_FOLD, T_DIST1, T_ROWS, T_PARITY, T_SIGN1, T_SIGN0, T_NUM };
 #define SDF_MARK(ctx, i) SDF_CUDA((ctx), cudaEventRecord((ctx)->tev[(i)], (ctx)->stream))
+#define SDF_MARK_ON(ctx, i, st) SDF_CUDA((ctx), cudaEventRecord((ctx)->tev[(i)], (st)))
+
+// Slots of ctx->h_scalars: device counts read back to size the next stage.  Page-locked, so the
+// read is an asynchronous copy the host waits for only when it needs the value.
+enum Scalar : int { S_ROW_TOTAL = 0, S_UNDECIDED, S_WINDING, S_NUM = 8 };
 
 #define SDF_TRY(expr)          \
   do {                         \
@@ -205,9 +213,22 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
                           bool device_ptrs);
 int ensure_ine(sdfgpu_ctx* ctx);
 int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, double* d_dist, double* d_xp);
-int run_signs(sdfgpu_ctx* ctx, const GridP& g, int min_rays, int max_rays, double conf_thresh, int use_winding,
-              const double* d_dist, double* d_sign, double* d_conf, double* d_sdf);
-int cub_scan_i32(sdfgpu_ctx* ctx, const int32_t* in, int32_t* out, int64_t n);
+// The sign stage in two parts on ctx->sign_stream: sign_begin enqueues the axis-row counting and
+// returns without waiting; sign_finish waits for that count and enqueues the rest (lists, parities,
+// vote, adaptive rays, winding).  Between the two the caller can enqueue the distance stage, which
+// then overlaps the sign stage on the GPU.  d_sign / d_conf receive the results.
+struct SignPlan {
+  int64_t Rx = 0, Ry = 0, Rz = 0, nrows = 0;
+  int32_t *row_cnt = nullptr, *row_off = nullptr, *row_cur = nullptr;
+};
+int sign_begin(sdfgpu_ctx* ctx, const GridP& g, SignPlan& P);
+int sign_finish(sdfgpu_ctx* ctx, const GridP& g, SignPlan& P, int min_rays, int max_rays, double conf_thresh,
+                int use_winding, double* d_sign, double* d_conf);
+int run_combine(sdfgpu_ctx* ctx, const GridP& g, const double* d_dist, const double* d_sign, double* d_sdf);
+// Exclusive scan of n int32 on stream st (the context stream when NULL), CUB temp storage in the
+// named scratch buffer (streams that may overlap use different names).
+int cub_scan_i32(sdfgpu_ctx* ctx, const int32_t* in, int32_t* out, int64_t n, cudaStream_t st = nullptr,
+                 const char* tmp_name = "cub_tmp_scan");
 int train_radius(sdfgpu_ctx* ctx, int coarse_n, int steps, int batch, float lr, uint64_t seed, float* final_loss);
 int set_radius_params(sdfgpu_ctx* ctx, const float* params, const double norm[4]);
 int get_radius_params(sdfgpu_ctx* ctx, float* params, double norm[4]);

@@ -377,12 +377,13 @@ int ensure_ine(sdfgpu_ctx* ctx) {
   return 0;
 }
 
-int cub_scan_i32(sdfgpu_ctx* ctx, const int32_t* in, int32_t* out, int64_t n) {
+int cub_scan_i32(sdfgpu_ctx* ctx, const int32_t* in, int32_t* out, int64_t n, cudaStream_t st, const char* tmp_name) {
+  if (!st) st = ctx->stream;
   size_t bytes = 0;
-  SDF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, (int)n, ctx->stream));
+  SDF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, (int)n, st));
   void* tmp;
-  SDF_TRY(scratch(ctx, "cub_tmp_scan", bytes, &tmp));
-  SDF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, (int)n, ctx->stream));
+  SDF_TRY(scratch(ctx, tmp_name, bytes, &tmp));
+  SDF_CUDA(ctx, cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, (int)n, st));
   return 0;
 }
 

@@ -21,6 +21,8 @@
 //     per node with a fixed-order block reduction.
 #include <cub/cub.cuh>
 
+#include <cstring>
+
 #include "common.cuh"
 
 namespace sdfgpu {
@@ -554,28 +556,42 @@ int upload_directions(sdfgpu_ctx* ctx, const double* dirs) {
   return 0;
 }
 
-int run_signs(sdfgpu_ctx* ctx, const GridP& g, int min_rays, int max_rays, double conf_thresh, int use_winding,
-              const double* d_dist, double* d_sign, double* d_conf, double* d_sdf) {
-  cudaStream_t st = ctx->stream;
+int sign_begin(sdfgpu_ctx* ctx, const GridP& g, SignPlan& P) {
+  cudaStream_t st = ctx->sign_stream;
+  const int64_t nel = ctx->mesh.nel;
+  const TriRec64* rec = buf<TriRec64>(ctx, "rec");
+  P.Rx = g.n[1] * g.n[2];
+  P.Ry = g.n[0] * g.n[2];
+  P.Rz = g.n[0] * g.n[1];
+  P.nrows = P.Rx + P.Ry + P.Rz;
+  if (P.nrows >= 0x7fffffffLL) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "grid has too many rows");
+  SDF_TRY(scratch_t(ctx, "row_cnt", (size_t)P.nrows + 1, &P.row_cnt));
+  SDF_TRY(scratch_t(ctx, "row_off", (size_t)P.nrows + 1, &P.row_off));
+  SDF_TRY(scratch_t(ctx, "row_cur", (size_t)P.nrows + 1, &P.row_cur));
+  SDF_CUDA(ctx, cudaMemsetAsync(P.row_cnt, 0, sizeof(int32_t) * (P.nrows + 1), st));
+  SDF_CUDA(ctx, cudaMemsetAsync(P.row_cur, 0, sizeof(int32_t) * (P.nrows + 1), st));
+  k_rows<<<grid_for(nel, 128), 128, 0, st>>>(rec, nel, g, P.Rx, P.Rx + P.Ry, false, P.row_cnt, nullptr, nullptr,
+                                             nullptr, nullptr, nullptr, ctx->d_counters);
+  SDF_KERNEL(ctx);
+  SDF_TRY(cub_scan_i32(ctx, P.row_cnt, P.row_off, P.nrows + 1, st, "cub_tmp_scan_sign"));
+  ctx->h_scalars[S_ROW_TOTAL] = -1;
+  SDF_CUDA(ctx, cudaMemcpyAsync(ctx->h_scalars + S_ROW_TOTAL, P.row_off + P.nrows, sizeof(int32_t),
+                                cudaMemcpyDeviceToHost, st));
+  SDF_CUDA(ctx, cudaEventRecord(ctx->ev_rows, st));
+  return 0;
+}
+
+int sign_finish(sdfgpu_ctx* ctx, const GridP& g, SignPlan& P, int min_rays, int max_rays, double conf_thresh,
+                int use_winding, double* d_sign, double* d_conf) {
+  cudaStream_t st = ctx->sign_stream;
   const MeshDev& M = ctx->mesh;
   const int64_t nel = M.nel;
   const TriRec64* rec = buf<TriRec64>(ctx, "rec");
-  const int64_t Rx = g.n[1] * g.n[2], Ry = g.n[0] * g.n[2], Rz = g.n[0] * g.n[1];
-  const int64_t nrows = Rx + Ry + Rz;
-  if (nrows >= 0x7fffffffLL) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "grid has too many rows");
-  int32_t *row_cnt, *row_off, *row_cur;
-  SDF_TRY(scratch_t(ctx, "row_cnt", (size_t)nrows + 1, &row_cnt));
-  SDF_TRY(scratch_t(ctx, "row_off", (size_t)nrows + 1, &row_off));
-  SDF_TRY(scratch_t(ctx, "row_cur", (size_t)nrows + 1, &row_cur));
-  SDF_CUDA(ctx, cudaMemsetAsync(row_cnt, 0, sizeof(int32_t) * (nrows + 1), st));
-  SDF_CUDA(ctx, cudaMemsetAsync(row_cur, 0, sizeof(int32_t) * (nrows + 1), st));
-  k_rows<<<grid_for(nel, 128), 128, 0, st>>>(rec, nel, g, Rx, Rx + Ry, false, row_cnt, nullptr, nullptr, nullptr,
-                                             nullptr, nullptr, ctx->d_counters);
-  SDF_KERNEL(ctx);
-  SDF_TRY(cub_scan_i32(ctx, row_cnt, row_off, nrows + 1));
-  int32_t total = 0;
-  SDF_CUDA(ctx, cudaMemcpyAsync(&total, row_off + nrows, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-  SDF_CUDA(ctx, cudaStreamSynchronize(st));
+  const int64_t Rx = P.Rx, Ry = P.Ry, nrows = P.nrows;
+  int32_t *row_cnt = P.row_cnt, *row_off = P.row_off, *row_cur = P.row_cur;
+  SDF_CUDA(ctx, cudaEventSynchronize(ctx->ev_rows));
+  int32_t total;
+  std::memcpy(&total, ctx->h_scalars + S_ROW_TOTAL, sizeof(int32_t));  // the low 4 bytes hold the int32
   if (total < 0) return fail(ctx, SDFGPU_ERR_CAPACITY, "more than 2^31 row hits");
   RowHit *hits_raw, *hits;
   unsigned long long *rkey, *rkey2;
@@ -596,7 +612,7 @@ int run_signs(sdfgpu_ctx* ctx, const GridP& g, int min_rays, int max_rays, doubl
     size_t tmp_bytes = 0;
     SDF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, rkey, rkey2, ridx, ridx2, total, 0, bits, st));
     void* tmp;
-    SDF_TRY(scratch(ctx, "cub_tmp", tmp_bytes, &tmp));
+    SDF_TRY(scratch(ctx, "cub_tmp_sign", tmp_bytes, &tmp));
     SDF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, rkey, rkey2, ridx, ridx2, total, 0, bits, st));
     k_gather_rows<<<grid_for(total, 256), 256, 0, st>>>(total, ridx2, hits_raw, hits);
     SDF_KERNEL(ctx);
@@ -606,14 +622,14 @@ int run_signs(sdfgpu_ctx* ctx, const GridP& g, int min_rays, int max_rays, doubl
   SDF_TRY(scratch_t(ctx, "par_y", (size_t)g.ngp, &py));
   SDF_TRY(scratch_t(ctx, "par_z", (size_t)g.ngp, &pz));
   const unsigned gp = grid_for(g.ngp, 256, 148 * 16);
-  SDF_MARK(ctx, T_ROWS);
+  SDF_MARK_ON(ctx, T_ROWS, st);
   k_axis_parity<0><<<gp, 256, 0, st>>>(g, 0, row_off, row_cnt, hits, px);
   SDF_KERNEL(ctx);
   k_axis_parity<1><<<gp, 256, 0, st>>>(g, Rx, row_off, row_cnt, hits, py);
   SDF_KERNEL(ctx);
   k_axis_parity<2><<<gp, 256, 0, st>>>(g, Rx + Ry, row_off, row_cnt, hits, pz);
   SDF_KERNEL(ctx);
-  SDF_MARK(ctx, T_PARITY);
+  SDF_MARK_ON(ctx, T_PARITY, st);
 
   int32_t *und, *wind;
   uint64_t *und_have, *und_par;
@@ -637,9 +653,10 @@ int run_signs(sdfgpu_ctx* ctx, const GridP& g, int min_rays, int max_rays, doubl
   V.counters = ctx->d_counters;
   k_vote<<<grid_for(g.ngp, 256, 148 * 16), 256, 0, st>>>(V);
   SDF_KERNEL(ctx);
-  int64_t nund = 0;
-  SDF_CUDA(ctx, cudaMemcpyAsync(&nund, ctx->d_counters + C_LIST_UNDECIDED, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  SDF_CUDA(ctx, cudaMemcpyAsync(ctx->h_scalars + S_UNDECIDED, ctx->d_counters + C_LIST_UNDECIDED, sizeof(int64_t),
+                                cudaMemcpyDeviceToHost, st));
   SDF_CUDA(ctx, cudaStreamSynchronize(st));
+  const int64_t nund = ctx->h_scalars[S_UNDECIDED];
   if (nund > 0) {
     // Rounds of the adaptive vote: decide what is decidable, cast the next requested rays.
     constexpr int kRounds = 12;  // initial rays + at most 8 batches reach the 36 directions
@@ -689,9 +706,10 @@ int run_signs(sdfgpu_ctx* ctx, const GridP& g, int min_rays, int max_rays, doubl
     SDF_KERNEL(ctx);
   }
   if (use_winding) {
-    int64_t nw = 0;
-    SDF_CUDA(ctx, cudaMemcpyAsync(&nw, ctx->d_counters + C_LIST_WINDING, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    SDF_CUDA(ctx, cudaMemcpyAsync(ctx->h_scalars + S_WINDING, ctx->d_counters + C_LIST_WINDING, sizeof(int64_t),
+                                  cudaMemcpyDeviceToHost, st));
     SDF_CUDA(ctx, cudaStreamSynchronize(st));
+    const int64_t nw = ctx->h_scalars[S_WINDING];
     if (nw > 0) {
       const int nchunks = (int)cdiv(nel, kWindChunk);
       double* partial;
@@ -703,10 +721,13 @@ int run_signs(sdfgpu_ctx* ctx, const GridP& g, int min_rays, int max_rays, doubl
       SDF_KERNEL(ctx);
     }
   }
-  if (d_sdf && d_dist) {
-    k_combine<<<grid_for(g.ngp, 256, 148 * 16), 256, 0, st>>>(g.ngp, d_dist, d_sign, d_sdf);
-    SDF_KERNEL(ctx);
-  }
+  return 0;
+}
+
+// sdf = dist .* sign (stl_to_sdf.jl:119) on the context stream.
+int run_combine(sdfgpu_ctx* ctx, const GridP& g, const double* d_dist, const double* d_sign, double* d_sdf) {
+  k_combine<<<grid_for(g.ngp, 256, 148 * 16), 256, 0, ctx->stream>>>(g.ngp, d_dist, d_sign, d_sdf);
+  SDF_KERNEL(ctx);
   return 0;
 }
 

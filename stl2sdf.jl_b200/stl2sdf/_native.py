@@ -285,9 +285,11 @@ class Context:
                                                  ctypes.c_void_p(conf_ptr or None)))
 
     def sdf_batch(self, meshes, mode=MODE_REF_RULE, min_rays=6, max_rays=30, confidence_threshold=0.6,
-                  use_winding_fallback=True, streams=8, autotune=True, want_parts=False):
+                  use_winding_fallback=True, streams=8, autotune=True, want_parts=False, out=None):
         """SDFs of many meshes, each on its own grid: meshes = [(X, IEN, origin, h, N), ...].
-        Returns one sdf array per mesh (with want_parts, (sdf, dist, sign, conf) per mesh)."""
+        Returns one sdf array per mesh (with want_parts, (sdf, dist, sign, conf) per mesh).  `out`
+        may supply the sdf arrays (contiguous float64, prod(N+1) each), e.g. views of page-locked
+        host memory, which the copies then reach by DMA."""
         keep, outs = [], []
         items = (BatchItem * max(1, len(meshes)))()
         for k, (X, IEN, origin, h, N) in enumerate(meshes):
@@ -295,15 +297,22 @@ class Context:
             IEN = np.ascontiguousarray(IEN, np.int64).reshape(-1, 3)
             N = np.ascontiguousarray(N, np.int64)
             ngp = int(np.prod(N + 1))
-            out = [np.empty(ngp)] + ([np.empty(ngp) for _ in range(3)] if want_parts else [None] * 3)
+            if out is not None:
+                o = out[k]
+                if o.dtype != np.float64 or not o.flags.c_contiguous or o.size != ngp:
+                    raise ValueError(f"out[{k}] must be a contiguous float64 array of {ngp} values")
+                first = o
+            else:
+                first = np.empty(ngp)
+            out_k = [first] + ([np.empty(ngp) for _ in range(3)] if want_parts else [None] * 3)
             keep += [X, IEN]
-            outs.append(out)
+            outs.append(out_k)
             it = items[k]
             it.X, it.nnp, it.IEN, it.nel = _d(X), X.shape[0], _i(IEN), IEN.shape[0]
             it.origin[:] = [float(v) for v in origin]
             it.h = float(h)
             it.N[:] = [int(v) for v in N]
-            it.sdf, it.dist, it.sign, it.conf = [(_d(a) if a is not None else None) for a in out]
+            it.sdf, it.dist, it.sign, it.conf = [(_d(a) if a is not None else None) for a in out_k]
         self._check(lib().sdfgpu_sdf_batch(self._p, items, len(meshes), int(mode), int(min_rays), int(max_rays),
                                            float(confidence_threshold), int(bool(use_winding_fallback)),
                                            int(streams), int(bool(autotune))))
