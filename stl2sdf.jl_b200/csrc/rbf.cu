@@ -13,7 +13,10 @@
 // c = K u, alpha = |r|^2 / (u . c), stop when |r| <= sqrt(eps(Float32)) |b| or after n
 // iterations; FP32 vectors, dot products accumulated in FP64 in a fixed order (deterministic).
 // The new search direction is formed on the fly inside the product (double-buffered), so one CG
-// iteration is two passes over the vectors.  The fine evaluation sums, per fine point, every
+// iteration is two passes over the vectors.  The loop runs as a CUDA graph of kGraphIters
+// iterations: the scalar kernel raises a device flag when the stopping rule holds, every kernel
+// after it returns at once, so the result is that of stopping exactly there, and the host reads
+// the flag once per graph launch instead of once per iteration.  The fine evaluation sums, per fine point, every
 // coarse node within the cut-off distance (the reference's 124-nearest query always contains
 // them all), with FP32 distances as the reference's KD-tree computes them and FP64 terms.
 #include <algorithm>
@@ -29,6 +32,11 @@ namespace {
 constexpr int kRbfMaxR = 4;      // stencil radius in cells (threshold >= exp(-16) ~ 1.1e-7)
 constexpr int kRbfBlocks = 592;  // fixed grid of the reduction kernels (4 per SM): fixed sum order
 constexpr int kRbfThreads = 256;
+constexpr int kGraphIters = 16;  // CG iterations per graph launch (even: the u buffers swap back)
+
+// Scalars of the CG loop (device): rr = |r|^2, beta, alpha, rr_prev, the stop flag (0/1), the
+// iteration count and the stopping bound on rr.
+enum CgScalar : int { CG_RR = 0, CG_BETA, CG_ALPHA, CG_RR_PREV, CG_DONE, CG_ITERS, CG_TOL2, CG_MAXIT, CG_NUM };
 
 struct Axis3 {
   const float* x[3];
@@ -64,9 +72,10 @@ __global__ void __launch_bounds__(kRbfThreads) k_rbf_matvec(Axis3 ax, const doub
                                                             const float* __restrict__ u_old, float* __restrict__ u_new,
                                                             float* __restrict__ c, const double* __restrict__ sc,
                                                             double* __restrict__ partial) {
+  if (sc[CG_DONE] != 0.0) return;  // converged in an earlier iteration of this graph
   const int64_t nx = ax.n[0], ny = ax.n[1], nz = ax.n[2], nxy = nx * ny, ngp = nxy * nz;
   const int W = 2 * R + 1;
-  const float beta = (float)sc[1];
+  const float beta = (float)sc[CG_BETA];
   double acc = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ngp; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t x = i % nx, y = (i / nx) % ny, z = i / nxy;
@@ -116,7 +125,8 @@ __global__ void __launch_bounds__(kRbfThreads) k_rbf_update(int64_t n, const dou
                                                             const float* __restrict__ u, const float* __restrict__ c,
                                                             float* __restrict__ x, float* __restrict__ r,
                                                             double* __restrict__ partial) {
-  const float alpha = (float)sc[2];
+  if (sc[CG_DONE] != 0.0) return;
+  const float alpha = (float)sc[CG_ALPHA];
   double acc = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     x[i] = fmaf(alpha, u[i], x[i]);
@@ -135,9 +145,11 @@ __global__ void __launch_bounds__(kRbfThreads) k_rbf_update(int64_t n, const dou
   }
 }
 
-// Scalars sc = {rr, beta, alpha, rr_prev}.  which = 0: alpha = rr / (u . c); which = 1: new rr and
-// the next beta = rr_new / rr_old.  One block, fixed order.
+// which = 0: alpha = rr / (u . c); which = 1: new rr, the next beta = rr_new / rr_old, one more
+// iteration counted and the stop flag raised when rr <= tol^2 or the iteration cap is reached;
+// which = 2: the initial rr = |b|^2 (no iteration, stop when b = 0).  One block, fixed order.
 __global__ void k_rbf_scalar(const double* __restrict__ partial, int count, double* sc, int which) {
+  if (which != 2 && sc[CG_DONE] != 0.0) return;
   __shared__ double red[kRbfThreads];
   double t = 0.0;
   for (int i = threadIdx.x; i < count; i += blockDim.x) t += partial[i];
@@ -150,11 +162,20 @@ __global__ void k_rbf_scalar(const double* __restrict__ partial, int count, doub
   if (threadIdx.x == 0) {
     const double sum = red[0];
     if (which == 0) {
-      sc[2] = sc[0] / sum;
+      sc[CG_ALPHA] = sc[CG_RR] / sum;
+    } else if (which == 1) {
+      sc[CG_RR_PREV] = sc[CG_RR];
+      sc[CG_RR] = sum;
+      sc[CG_BETA] = sum / sc[CG_RR_PREV];
+      sc[CG_ITERS] += 1.0;
+      if (!(sum > sc[CG_TOL2]) || sc[CG_ITERS] >= sc[CG_MAXIT]) sc[CG_DONE] = 1.0;
     } else {
-      sc[3] = sc[0];
-      sc[0] = sum;
-      sc[1] = sum / sc[3];
+      // IterativeSolvers: prev_residual = 1 at the start, so the first beta is |b|^2 (u is 0)
+      sc[CG_RR] = sum;
+      sc[CG_RR_PREV] = 1.0;
+      sc[CG_BETA] = sum;
+      sc[CG_TOL2] = (double)FLT_EPSILON * sum;  // (sqrt(eps(Float32)) |b|)^2
+      if (!(sum > sc[CG_TOL2])) sc[CG_DONE] = 1.0;
     }
   }
 }
@@ -280,7 +301,7 @@ extern "C" int sdfgpu_rbf_smoothing(sdfgpu_ctx* ctx, const double aabb_min[3], c
   SDF_TRY(scratch_t(ctx, "rbf_c", (size_t)n, &c));
   SDF_TRY(scratch_t(ctx, "rbf_out", (size_t)m, &out));
   SDF_TRY(scratch_t(ctx, "rbf_part", kRbfBlocks, &part));
-  SDF_TRY(scratch_t(ctx, "rbf_sc", 4, &sc));
+  SDF_TRY(scratch_t(ctx, "rbf_sc", CG_NUM, &sc));
   SDF_TRY(scratch_t(ctx, "rbf_mx", 1, &mx));
   SDF_CUDA(ctx, cudaMemcpyAsync(dc, hc.data(), sizeof(float) * hc.size(), cudaMemcpyHostToDevice, st));
   SDF_CUDA(ctx, cudaMemcpyAsync(df, hf.data(), sizeof(float) * hf.size(), cudaMemcpyHostToDevice, st));
@@ -298,38 +319,65 @@ extern "C" int sdfgpu_rbf_smoothing(sdfgpu_ctx* ctx, const double aabb_min[3], c
   int iters = 0;
   double res = 0.0;
   if (interpolation) {
-    // x = 0, r = b, u = 0, rr = |b|^2, beta = rr / 1 (u is zero, so the first direction is r)
+    // x = 0, r = b, u = 0; |b|^2 through the update's reduction with alpha = 0 (x and r unchanged)
     SDF_CUDA(ctx, cudaMemsetAsync(x, 0, sizeof(float) * n, st));
     SDF_CUDA(ctx, cudaMemsetAsync(u0, 0, sizeof(float) * n, st));
     SDF_CUDA(ctx, cudaMemcpyAsync(r, b, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
-    // |b|^2 through the update's reduction with alpha = 0 (x and r unchanged)
-    double h_sc[4] = {1.0, 0.0, 0.0, 1.0};
+    double h_sc[CG_NUM] = {0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, (double)n};
     SDF_CUDA(ctx, cudaMemcpyAsync(sc, h_sc, sizeof(h_sc), cudaMemcpyHostToDevice, st));
-    k_rbf_update<<<kRbfBlocks, kRbfThreads, 0, st>>>(n, sc, u0, u0, x, r, part);  // alpha = 0: x, r unchanged
+    k_rbf_update<<<kRbfBlocks, kRbfThreads, 0, st>>>(n, sc, u0, u0, x, r, part);
     SDF_KERNEL(ctx);
-    k_rbf_scalar<<<1, kRbfThreads, 0, st>>>(part, kRbfBlocks, sc, 1);  // sc[0] = |b|^2, beta = |b|^2
+    k_rbf_scalar<<<1, kRbfThreads, 0, st>>>(part, kRbfBlocks, sc, 2);
     SDF_KERNEL(ctx);
-    double rr = 0.0;
-    SDF_CUDA(ctx, cudaMemcpyAsync(&rr, sc, sizeof(double), cudaMemcpyDeviceToHost, st));
-    SDF_CUDA(ctx, cudaStreamSynchronize(st));
-    const double tol = std::sqrt((double)FLT_EPSILON) * std::sqrt(rr);
-    float* ua = u0;
-    float* ub = u1;
-    while (!(iters >= n || std::sqrt(rr) <= tol)) {
+    // kGraphIters iterations captured once: matvec (u0 -> u1), alpha, update, rr; then u1 -> u0.
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    auto release = [&]() {
+      if (exec) cudaGraphExecDestroy(exec);
+      if (graph) cudaGraphDestroy(graph);
+    };
+    SDF_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    bool cap_ok = true;
+    for (int k = 0; k < kGraphIters && cap_ok; ++k) {
+      float* ua = (k & 1) ? u1 : u0;
+      float* ub = (k & 1) ? u0 : u1;
       k_rbf_matvec<<<kRbfBlocks, kRbfThreads, 0, st>>>(ac, kt, R, threshold, r, ua, ub, c, sc, part);
-      SDF_KERNEL(ctx);
       k_rbf_scalar<<<1, kRbfThreads, 0, st>>>(part, kRbfBlocks, sc, 0);
-      SDF_KERNEL(ctx);
       k_rbf_update<<<kRbfBlocks, kRbfThreads, 0, st>>>(n, sc, ub, c, x, r, part);
-      SDF_KERNEL(ctx);
       k_rbf_scalar<<<1, kRbfThreads, 0, st>>>(part, kRbfBlocks, sc, 1);
-      SDF_KERNEL(ctx);
-      SDF_CUDA(ctx, cudaMemcpyAsync(&rr, sc, sizeof(double), cudaMemcpyDeviceToHost, st));
-      SDF_CUDA(ctx, cudaStreamSynchronize(st));
-      std::swap(ua, ub);
-      ++iters;
-      if (!std::isfinite(rr)) return fail(ctx, SDFGPU_ERR_CUDA, "rbf_smoothing: CG diverged (non-finite residual)");
+      cap_ok = cudaGetLastError() == cudaSuccess;
     }
+    cudaError_t ce = cudaStreamEndCapture(st, &graph);
+    if (!cap_ok || ce != cudaSuccess) {
+      release();
+      return fail(ctx, SDFGPU_ERR_CUDA, std::string("rbf_smoothing: CG graph capture failed: ") + cudaGetErrorString(ce));
+    }
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    if (ce != cudaSuccess) {
+      release();
+      return fail(ctx, SDFGPU_ERR_CUDA, std::string("rbf_smoothing: cudaGraphInstantiate: ") + cudaGetErrorString(ce));
+    }
+    ctx->launches += 4 * kGraphIters;
+    static_assert((int)CG_NUM <= (int)S_NUM, "the CG scalars are read back through the context's page-locked slots");
+    double* h_out = reinterpret_cast<double*>(ctx->h_scalars);  // page-locked: read back per launch
+    const int64_t max_launches = n / kGraphIters + 2;
+    for (int64_t l = 0;; ++l) {
+      ce = cudaGraphLaunch(exec, st);
+      if (ce == cudaSuccess) ce = cudaMemcpyAsync(h_out, sc, sizeof(double) * CG_NUM, cudaMemcpyDeviceToHost, st);
+      if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+      if (ce != cudaSuccess) {
+        release();
+        return fail(ctx, SDFGPU_ERR_CUDA, std::string("rbf_smoothing: CG graph: ") + cudaGetErrorString(ce));
+      }
+      if (!std::isfinite(h_out[CG_RR])) {
+        release();
+        return fail(ctx, SDFGPU_ERR_CUDA, "rbf_smoothing: CG diverged (non-finite residual)");
+      }
+      if (h_out[CG_DONE] != 0.0 || l >= max_launches) break;
+    }
+    release();
+    iters = (int)h_out[CG_ITERS];
+    const double rr = h_out[CG_RR];
     res = std::sqrt(rr);
     weights = x;
   }
