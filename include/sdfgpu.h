@@ -92,7 +92,8 @@ typedef struct sdfgpu_stats {
   double rho_max;                 /* max vertex distance from a triangle centroid */
   double ms_distance;             /* device time of the distance stage (ms) */
   double ms_sign;                 /* device time of the sign stage (ms) */
-  double ms_mesh;                 /* device time of the last set_mesh (ms) */
+  double ms_mesh;                 /* device time of the last set_mesh up to the triangle records (ms); the LBVH
+                                     build runs beside the next call's distance stage */
   int64_t launches;               /* kernels of this library launched by the last call (CUB excluded) */
   int64_t mesh_launches;          /* same, for the last set_mesh */
   double ms_tiles;                /* (tile, triangle) pair build + sort */

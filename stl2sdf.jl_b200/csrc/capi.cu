@@ -260,6 +260,8 @@ int run_all(sdfgpu_ctx* ctx, const GridP& g, bool want_dist, bool want_sign, int
     SDF_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
   }
   if (want_dist && want_sign && d_sdf) SDF_TRY(run_combine(ctx, g, d_dist, d_sign, d_sdf));
+  // a call ends after the mesh's LBVH build too, whether or not this call used it
+  SDF_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_bvh, 0));
   SDF_TRY(finish_counters(ctx, g));
   auto span = [&](int a, int b, double* out) -> int {
     float ms = 0.f;
@@ -373,7 +375,9 @@ int sdfgpu_create(const sdfgpu_opts* opts, sdfgpu_ctx** out) {
   if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail("cudaStreamCreate", e);
   if ((e = cudaStreamCreateWithFlags(&ctx->sign_stream, cudaStreamNonBlocking)) != cudaSuccess)
     return bail("cudaStreamCreate", e);
-  for (cudaEvent_t* ev : {&ctx->ev_fork, &ctx->ev_join, &ctx->ev_rows})
+  if ((e = cudaStreamCreateWithFlags(&ctx->bvh_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return bail("cudaStreamCreate", e);
+  for (cudaEvent_t* ev : {&ctx->ev_fork, &ctx->ev_join, &ctx->ev_rows, &ctx->ev_mesh, &ctx->ev_bvh})
     if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return bail("cudaEventCreate", e);
   if ((e = cudaHostAlloc((void**)&ctx->h_scalars, sizeof(int64_t) * S_NUM, cudaHostAllocDefault)) != cudaSuccess)
     return bail("cudaHostAlloc", e);
@@ -400,6 +404,7 @@ int sdfgpu_destroy(sdfgpu_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->sign_stream) cudaStreamSynchronize(ctx->sign_stream);
+  if (ctx->bvh_stream) cudaStreamSynchronize(ctx->bvh_stream);
   for (auto& kv : ctx->bufs)
     if (kv.second.p) cudaFree(kv.second.p);
   if (ctx->d_counters) cudaFree(ctx->d_counters);
@@ -407,8 +412,9 @@ int sdfgpu_destroy(sdfgpu_ctx* ctx) {
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : ctx->tev)
     if (ev) cudaEventDestroy(ev);
-  for (cudaEvent_t ev : {ctx->ev_fork, ctx->ev_join, ctx->ev_rows})
+  for (cudaEvent_t ev : {ctx->ev_fork, ctx->ev_join, ctx->ev_rows, ctx->ev_mesh, ctx->ev_bvh})
     if (ev) cudaEventDestroy(ev);
+  if (ctx->bvh_stream) cudaStreamDestroy(ctx->bvh_stream);
   if (ctx->h_scalars) cudaFreeHost(ctx->h_scalars);
   if (ctx->sign_stream) cudaStreamDestroy(ctx->sign_stream);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);

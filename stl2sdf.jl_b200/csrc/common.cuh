@@ -108,7 +108,10 @@ struct sdfgpu_ctx {
   int64_t launches = 0;  // kernels of this library launched since the last reset
   cudaEvent_t tev[8] = {};  // stage timestamps, see sdfgpu::Stage
   cudaStream_t sign_stream = nullptr;    // the sign stage runs here, beside the distance stage
+  cudaStream_t bvh_stream = nullptr;     // the LBVH build runs here, beside the distance stage
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_rows = nullptr;
+  cudaEvent_t ev_mesh = nullptr;         // triangle records ready (on the context stream)
+  cudaEvent_t ev_bvh = nullptr;          // LBVH of the current mesh complete (on bvh_stream)
   int64_t* h_scalars = nullptr;          // page-locked host slots for sizing reads (see Scalar)
   std::vector<sdfgpu_ctx*> workers;      // batch workers (batch.cu), created on first use
   std::map<int64_t, uint32_t> tuned;     // autotuner: size class -> packed tile (batch.cu)

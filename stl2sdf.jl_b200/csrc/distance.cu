@@ -718,6 +718,7 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
   const float pad = 2.0e-6f * E;
 
   if (mode == SDFGPU_MODE_UNBOUNDED) {
+    SDF_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_bvh, 0));  // the search walks the LBVH
     float* radius = nullptr;
     if (use_learned) {
       // r = (dhat (1 + alpha) + beta * coarse spacing / s) s: a margin for the network's error and
@@ -840,6 +841,7 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
       K.dist = d_dist;
       K.xp = d_xp;
       K.counters = ctx->d_counters;
+      SDF_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_bvh, 0));  // the fallback walks the LBVH
       k_knn_fallback<<<grid_for(g.ngp, 128, 148 * 16), 128, 0, st>>>(K);
       SDF_KERNEL(ctx);
     }

@@ -138,16 +138,26 @@ __device__ __forceinline__ unsigned expand_bits10(unsigned v) {
   return v;
 }
 
+// 30-bit Morton code of each centroid and the triangle index; a stable sort of the codes (index as
+// the value) orders the triangles exactly as the unique 64-bit keys (code << 32 | index) would, in
+// half the radix passes.
 __global__ void k_morton(const float4* __restrict__ c32, int64_t nel, float lox, float loy, float loz, float inv,
-                         unsigned long long* __restrict__ keys) {
+                         uint32_t* __restrict__ code, int32_t* __restrict__ idx) {
   for (int64_t el = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; el < nel; el += (int64_t)gridDim.x * blockDim.x) {
     const float4 c = c32[el];
     const float fx = fminf(fmaxf((c.x - lox) * inv, 0.f), 1023.f);
     const float fy = fminf(fmaxf((c.y - loy) * inv, 0.f), 1023.f);
     const float fz = fminf(fmaxf((c.z - loz) * inv, 0.f), 1023.f);
-    const unsigned m = (expand_bits10((unsigned)fx) << 2) | (expand_bits10((unsigned)fy) << 1) | expand_bits10((unsigned)fz);
-    keys[el] = ((unsigned long long)m << 32) | (unsigned long long)el;
+    code[el] = (expand_bits10((unsigned)fx) << 2) | (expand_bits10((unsigned)fy) << 1) | expand_bits10((unsigned)fz);
+    idx[el] = (int32_t)el;
   }
+}
+
+// The sorted unique keys (code << 32 | index) the hierarchy build splits on.
+__global__ void k_pack_keys(const uint32_t* __restrict__ code, const int32_t* __restrict__ idx, int n,
+                            unsigned long long* __restrict__ keys) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    keys[i] = ((unsigned long long)code[i] << 32) | (unsigned long long)(uint32_t)idx[i];
 }
 
 __device__ __forceinline__ int kdelta(const unsigned long long* __restrict__ k, int n, int i, int j) {
@@ -250,6 +260,8 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
   ctx->has_mesh = false;
   ctx->mesh.ine_ready = false;
   ctx->launches = 0;
+  // the previous mesh's LBVH build reads the buffers rewritten below
+  SDF_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_bvh, 0));
   SDF_CUDA(ctx, cudaEventRecord(ctx->ev[4], st));
 
   double* dX;
@@ -307,12 +319,16 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
                                                  c32, box32, bb + 7);
   SDF_KERNEL(ctx);
 
-  // LBVH
+  // LBVH, on its own stream: only the unbounded search, the 3-nearest-vertex fallback and the
+  // adaptive rays read it, and they wait for ev_bvh; the tile lists and the fold do not, so the
+  // build overlaps the distance stage of the next call.
+  SDF_CUDA(ctx, cudaEventRecord(ctx->ev_mesh, st));
+  cudaStream_t sb = ctx->bvh_stream;
+  SDF_CUDA(ctx, cudaStreamWaitEvent(sb, ctx->ev_mesh, 0));
   const int n = (int)nel;
-  unsigned long long *keys, *keys2;
+  unsigned long long* keys2;
   BNode* nodes;
   int32_t *int_parent, *leaf_parent, *flags, *leaf_prim;
-  SDF_TRY(scratch_t(ctx, "keys", (size_t)n, &keys));
   SDF_TRY(scratch_t(ctx, "keys2", (size_t)n, &keys2));
   SDF_TRY(scratch_t(ctx, "nodes", (size_t)std::max(1, n - 1), &nodes));
   SDF_TRY(scratch_t(ctx, "int_parent", (size_t)n, &int_parent));
@@ -320,27 +336,36 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
   SDF_TRY(scratch_t(ctx, "flags", (size_t)n, &flags));
   SDF_TRY(scratch_t(ctx, "leaf_prim", (size_t)n, &leaf_prim));
   if (n == 1) {
-    k_single_root<<<1, 1, 0, st>>>(box32, nodes, leaf_prim);
+    k_single_root<<<1, 1, 0, sb>>>(box32, nodes, leaf_prim);
     SDF_KERNEL(ctx);
   } else {
     const float lox = (float)(M.bmin[0] - M.center[0]), loy = (float)(M.bmin[1] - M.center[1]),
                 loz = (float)(M.bmin[2] - M.center[2]);
     const double ext = std::max(M.bmax[0] - M.bmin[0], std::max(M.bmax[1] - M.bmin[1], M.bmax[2] - M.bmin[2]));
     const float inv = ext > 0 ? (float)(1024.0 / ext) : 1.0f;
-    k_morton<<<grid_for(nel, 256), 256, 0, st>>>(c32, nel, lox, loy, loz, inv, keys);
+    uint32_t *code, *code2;
+    int32_t *idx, *idx2;
+    SDF_TRY(scratch_t(ctx, "mcode", (size_t)n, &code));
+    SDF_TRY(scratch_t(ctx, "mcode2", (size_t)n, &code2));
+    SDF_TRY(scratch_t(ctx, "midx", (size_t)n, &idx));
+    SDF_TRY(scratch_t(ctx, "midx2", (size_t)n, &idx2));
+    k_morton<<<grid_for(nel, 256), 256, 0, sb>>>(c32, nel, lox, loy, loz, inv, code, idx);
     SDF_KERNEL(ctx);
     size_t tmp_bytes = 0;
-    SDF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, keys, keys2, n, 0, 62, st));
+    SDF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, code, code2, idx, idx2, n, 0, 30, sb));
     void* tmp;
-    SDF_TRY(scratch(ctx, "cub_tmp", tmp_bytes, &tmp));
-    SDF_CUDA(ctx, cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, keys, keys2, n, 0, 62, st));
-    SDF_CUDA(ctx, cudaMemsetAsync(int_parent, 0xff, sizeof(int32_t) * n, st));
-    SDF_CUDA(ctx, cudaMemsetAsync(flags, 0, sizeof(int32_t) * n, st));
-    k_karras<<<grid_for(n - 1, 256), 256, 0, st>>>(keys2, n, nodes, int_parent, leaf_parent);
+    SDF_TRY(scratch(ctx, "cub_tmp_bvh", tmp_bytes, &tmp));
+    SDF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, code, code2, idx, idx2, n, 0, 30, sb));
+    k_pack_keys<<<grid_for(n, 256), 256, 0, sb>>>(code2, idx2, n, keys2);
     SDF_KERNEL(ctx);
-    k_refit<<<grid_for(n, 256), 256, 0, st>>>(keys2, box32, n, nodes, int_parent, leaf_parent, flags, leaf_prim);
+    SDF_CUDA(ctx, cudaMemsetAsync(int_parent, 0xff, sizeof(int32_t) * n, sb));
+    SDF_CUDA(ctx, cudaMemsetAsync(flags, 0, sizeof(int32_t) * n, sb));
+    k_karras<<<grid_for(n - 1, 256), 256, 0, sb>>>(keys2, n, nodes, int_parent, leaf_parent);
+    SDF_KERNEL(ctx);
+    k_refit<<<grid_for(n, 256), 256, 0, sb>>>(keys2, box32, n, nodes, int_parent, leaf_parent, flags, leaf_prim);
     SDF_KERNEL(ctx);
   }
+  SDF_CUDA(ctx, cudaEventRecord(ctx->ev_bvh, sb));
   unsigned long long hrho = 0;
   SDF_CUDA(ctx, cudaMemcpyAsync(&hrho, bb + 7, sizeof(hrho), cudaMemcpyDeviceToHost, st));
   SDF_CUDA(ctx, cudaEventRecord(ctx->ev[5], st));

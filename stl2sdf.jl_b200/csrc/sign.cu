@@ -670,6 +670,7 @@ int sign_finish(sdfgpu_ctx* ctx, const GridP& g, SignPlan& P, int min_rays, int 
     SDF_TRY(scratch_t(ctx, "rq_cnt", (size_t)kRounds + 1, &rq_cnt));
     SDF_CUDA(ctx, cudaMemsetAsync(done, 0, (size_t)nund, st));
     SDF_CUDA(ctx, cudaMemsetAsync(rq_cnt, 0, sizeof(int64_t) * (kRounds + 1), st));
+    SDF_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_bvh, 0));  // the adaptive rays walk the LBVH
     RayArgs R;
     R.g = g;
     R.nodes = buf<BNode>(ctx, "nodes");
