@@ -136,7 +136,7 @@ def cpu_baseline(X, IEN, g, budget_s=12.0, seed=42):
             "sample": f"{nodes.shape[0]} seeded (seed {seed}) uniform grid nodes of the workload, distance+sign, {dt:.1f} s"}
 
 
-def distance_variants(ctx, X, IEN, g, reps=3):
+def distance_variants(ctx, X, IEN, g, reps=3, work=None, peak_tflops=None):
     """Distance-stage throughput (device time of sdfgpu_distances, mesh resident) of the modes the
     metric compares: the reference rule (clamped), the true minimum clamped to h, the plain unbounded
     search and the learned-radius unbounded search (bit-identical to plain), plus the network's
@@ -171,6 +171,15 @@ def distance_variants(ctx, X, IEN, g, reps=3):
                                      "margin": "r = (dhat (1 + 0.1) + 1 coarse spacing) s",
                                      "bvh_visits_per_node": st["bvh_visits"] / g["ngp"]})
     out["learned_vs_plain_unbounded"] = out["plain_unbounded"]["ms"] / out["learned_unbounded"]["ms"]
+    if work is not None and peak_tflops:
+        # FP32 roofline of the distance stage alone: F_pt |D*| per node (clamped forms) or F_pt |D*_u|
+        # (unbounded forms), against the measured FP32 peak
+        for k, w in (("ref_rule", work["mean_W_dist_flop"]), ("exact_h_bounded", work["mean_W_dist_flop"]),
+                     ("plain_unbounded", work["mean_W_dist_unbounded_flop"]),
+                     ("learned_unbounded", work["mean_W_dist_unbounded_flop"])):
+            bound = peak_tflops * 1e12 / w
+            out[k]["roofline_fp32"] = {"mean_W_flop_per_node": w, "roofline_nodes_per_s": bound,
+                                       "frac": out[k]["nodes_per_s"] / bound}
     return out
 
 
@@ -280,6 +289,9 @@ def run_batch(args, rank, world, local):
         dt, launches = timed(args.steps, streams=args.streams, autotune=True)
     st = ctx.stats()
     one, _ = timed(1, streams=1, autotune=False)  # same batch, one stream, default tile
+    # the same batch with the folds of all meshes in one persistent launch inside a CUDA graph
+    ctx.sdf_batch(mine, out=outs, streams=args.streams, autotune=True, persistent=True)  # buffers
+    pers, _ = timed(max(1, min(args.steps, 3)), streams=args.streams, autotune=True, persistent=True)
     total = sum(ngps)
     value = total * args.steps / dt
     line = {
@@ -296,6 +308,9 @@ def run_batch(args, rank, world, local):
                 "d2h_bytes_per_step": int(8 * sum(ngps[i] for i in plan[rank]))},
         "gpu_launches": int(launches),
         "single_stream_default_tile": {"value": total / one, "s": one},
+        "persistent_graph_form": {"value": total * max(1, min(args.steps, 3)) / pers,
+                                  "note": "sdfgpu_sdf_batch_ex(persistent=1): every fold in one persistent launch, "
+                                          "captured with the epilogues in one CUDA graph"},
         "first_call_s": t_tune,
         "stages_ms_summed": {k: st[k] for k in ("ms_mesh", "ms_tiles", "ms_fold", "ms_rows", "ms_parity", "ms_vote")},
         "counters_summed": {k: st[k] for k in ("tile_pairs", "fp64_evals", "row_hits", "undecided_nodes", "extra_rays",
@@ -513,7 +528,8 @@ def main():
         "wall_s": wall,
     }
     if not args.no_variants:
-        line["distance_variants"] = distance_variants(ctx, X, IEN, g)
+        line["distance_variants"] = distance_variants(ctx, X, IEN, g, work=wm,
+                                                      peak_tflops=roof32["peak"] if roof32 else None)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(X, IEN, g)
     if dist_on:

@@ -218,6 +218,19 @@ int sdfgpu_sdf_batch(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count, i
                      int32_t max_rays, double confidence_threshold, int32_t use_winding_fallback, int32_t streams,
                      int32_t autotune);
 
+/* sdfgpu_sdf_batch with the choice of how the reference-rule and h-bounded modes run (results are
+ * the same either way).  persistent = 0: each item runs the whole per-mesh pipeline on one of the
+ * worker streams (sdfgpu_sdf_batch does this).  persistent = 1: the workers first prepare every
+ * item (mesh, LBVH, tile lists, sign stage) in item-private buffers; then one CUDA graph runs the
+ * folds of all items in a single persistent kernel launch (CTAs striding over the batch's (item,
+ * tile) work list, every item with its own tile) followed by each item's nearest-vertex fallback
+ * and combine on the worker streams side by side; then the fields are copied out.  Items go to the
+ * workers by a fixed longest-processing-time assignment, so repeated batches reuse their buffers.
+ * Unbounded batches always run per item. */
+int sdfgpu_sdf_batch_ex(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count, int32_t mode, int32_t min_rays,
+                        int32_t max_rays, double confidence_threshold, int32_t use_winding_fallback, int32_t streams,
+                        int32_t autotune, int32_t persistent);
+
 /* Tile autotuner for the distance stage (the reference has no counterpart).  Times the current mesh
  * on the grid (origin, h, N) in `mode` with each built-in tile shape (nodes per CTA along x, y, z:
  * 4x4x4, 8x4x2, 4x4x2, 8x4x4, 4x4x8, 8x8x4), keeps the fastest as ctx's tile and writes it to

@@ -65,7 +65,7 @@ def lib():
         L.oracle_barycentric.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp]
         L.oracle_winding.argtypes = [_dp, ctypes.c_int64, _i64p, ctypes.c_int64, _dp, ctypes.c_int64, _dp, _dp, ctypes.c_int]
         L.oracle_work_model.argtypes = [_dp, ctypes.c_int64, _i64p, ctypes.c_int64, _dp, ctypes.c_double, _i64p, _i64p,
-                                        ctypes.c_int64, _i64p, _i64p, _i64p, _i32p, ctypes.c_int]
+                                        ctypes.c_int64, _i64p, _i64p, _i64p, _i32p, _i64p, ctypes.c_int]
         L.oracle_max_threads.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -178,7 +178,7 @@ def winding(X, IEN, pts, nthreads=0):
 
 
 def work_model(X, IEN, origin, h, N, nodes, nthreads=0):
-    """Per-node algorithmic work counts: dict(nD, nrow (k x 3), nextra, rays); see oracle_work_model."""
+    """Per-node algorithmic work counts: dict(nD, nD_unb, nrow (k x 3), nextra, rays); see oracle_work_model."""
     X, IEN = _mesh_arrays(X, IEN)
     N = np.asarray(N, dtype=np.int64)
     origin = np.asarray(origin, dtype=np.float64)
@@ -186,13 +186,14 @@ def work_model(X, IEN, origin, h, N, nodes, nthreads=0):
     k = nodes.shape[0]
     nD = np.empty(k, np.int64); nrow = np.empty((k, 3), np.int64); nextra = np.empty(k, np.int64)
     rays = np.empty(k, np.int32)
+    nDu = np.empty(k, np.int64)
     rc = lib().oracle_work_model(_d(X), X.shape[0], IEN.ctypes.data_as(_i64p), IEN.shape[0], _d(origin), float(h),
                                  N.ctypes.data_as(_i64p), nodes.ctypes.data_as(_i64p), k, nD.ctypes.data_as(_i64p),
                                  nrow.ctypes.data_as(_i64p), nextra.ctypes.data_as(_i64p), rays.ctypes.data_as(_i32p),
-                                 int(nthreads))
+                                 nDu.ctypes.data_as(_i64p), int(nthreads))
     if rc != 0:
         raise ValueError("oracle_work_model failed")
-    return dict(nD=nD, nrow=nrow, nextra=nextra, rays=rays)
+    return dict(nD=nD, nD_unb=nDu, nrow=nrow, nextra=nextra, rays=rays)
 
 
 def max_threads() -> int:

@@ -883,7 +883,7 @@ int oracle_winding(const double* X, int64_t nnp, const int64_t* IEN, int64_t nel
 int oracle_work_model(const double* X, int64_t nnp, const int64_t* IEN, int64_t nel,
                       const double origin[3], double h, const int64_t N[3], const int64_t* nodes,
                       int64_t nnodes, int64_t* nD, int64_t* nrow, int64_t* nextra, int32_t* rays,
-                      int nthreads) {
+                      int64_t* nD_unb, int nthreads) {
   if (nel <= 0 || nnp <= 0 || !nodes) return 1;
   Grid g;
   if (!grid_from(origin, h, N, g)) return 1;
@@ -902,22 +902,27 @@ int oracle_work_model(const double* X, int64_t nnp, const int64_t* IEN, int64_t 
       V3 proj;
       int fl = 0;
       const double dt = eval_node(M, g, p, MODE_UNBOUNDED, proj, fl, cand);
-      const double r = std::min(dt, g.h);
-      cand.clear();
-      query_ball(M.bvh, p, r, cand);
-      int64_t c = 0;
-      for (int64_t el : cand) {
-        const Tri& t = M.T[(size_t)el];
-        const double lo[3] = {t.bmin.x, t.bmin.y, t.bmin.z}, hi[3] = {t.bmax.x, t.bmax.y, t.bmax.z};
-        const double pc[3] = {p.x, p.y, p.z};
-        double s2 = 0.0;
-        for (int a = 0; a < 3; ++a) {
-          const double dd = pc[a] < lo[a] ? lo[a] - pc[a] : (pc[a] > hi[a] ? pc[a] - hi[a] : 0.0);
-          s2 += dd * dd;
+      // triangles whose AABB lies within radius r of p
+      auto count_within = [&](double r) {
+        cand.clear();
+        query_ball(M.bvh, p, r, cand);
+        int64_t c = 0;
+        for (int64_t el : cand) {
+          const Tri& t = M.T[(size_t)el];
+          const double lo[3] = {t.bmin.x, t.bmin.y, t.bmin.z}, hi[3] = {t.bmax.x, t.bmax.y, t.bmax.z};
+          const double pc[3] = {p.x, p.y, p.z};
+          double s2 = 0.0;
+          for (int a = 0; a < 3; ++a) {
+            const double dd = pc[a] < lo[a] ? lo[a] - pc[a] : (pc[a] > hi[a] ? pc[a] - hi[a] : 0.0);
+            s2 += dd * dd;
+          }
+          if (s2 <= r * r) ++c;
         }
-        if (s2 <= r * r) ++c;
-      }
-      nD[q] = c;
+        return c;
+      };
+      nD[q] = count_within(std::min(dt, g.h));
+      // the unclamped form: every triangle a box-pruned search for the true minimum must look at
+      if (nD_unb) nD_unb[q] = dt <= g.h ? nD[q] : count_within(dt);
       // grid lines: both coordinates other than a inside the triangle's box
       const double pc[3] = {p.x, p.y, p.z};
       for (int a = 0; a < 3; ++a) {

@@ -16,7 +16,9 @@ must do per node:
 * F_PT, F_MT: FP32 FLOPs (FMA = 2, division = 1) of the closed-form point-triangle distance
   (three segment distances, three edge-side tests, the plane distance) and of Moller-Trumbore.
 
-Roofline nodes/s = P_fp32 / mean W.  Results go to profiles/roofline.json, which bench.py reads.
+Roofline nodes/s = P_fp32 / mean W.  The distance stage alone is bounded by F_PT |D*(p)|, and the
+unclamped (unbounded) distance by F_PT |D*_u(p)| with D*_u(p) the triangles whose AABB lies within
+d_true(p) of p.  Results go to profiles/roofline.json, which bench.py reads.
 
     python oracle/work_model.py [workload ...]      (default: icosphere torus128 blobs256 gyroid320)
 """
@@ -54,6 +56,9 @@ def model(name: str) -> dict:
     ray_share = (c["nrow"] / n_line[None, :]).sum(axis=1) + c["nextra"]
     W = F_PT * c["nD"] + F_MT * ray_share
     return {
+        "mean_W_dist_flop": float(F_PT * c["nD"].mean()),
+        "mean_W_dist_unbounded_flop": float(F_PT * c["nD_unb"].mean()),
+        "mean_Dstar_unbounded": float(c["nD_unb"].mean()),
         "workload": name, "description": desc, "ngp": ngp, "nel": int(IEN.shape[0]),
         "sample": f"{nodes.shape[0]} nodes" + (" (whole grid)" if nodes.shape[0] == ngp else f", uniform, seed {SEED}"),
         "F_pt": F_PT, "F_mt": F_MT, "mean_W_flop": float(W.mean()),

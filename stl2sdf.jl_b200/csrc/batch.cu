@@ -1,14 +1,25 @@
 // batch.cu -- many meshes per call (sdfgpu_sdf_batch) and the tile autotuner (sdfgpu_autotune).
 //
 // A batch is a queue of (mesh, grid) items drained by worker contexts, one host thread and one
-// CUDA stream each.  The per-mesh pipeline has host-sized stages (the (tile, triangle) pair count,
-// the axis-row hit count, the undecided-node count), so one mesh alone leaves the GPU idle while
-// its host thread waits; several workers fill those gaps with the kernels of other meshes.  Items
-// are taken largest first (longest-processing-time order), which also makes each worker's scratch
-// buffers reach their final size on its first item, so later items allocate nothing.
+// CUDA stream each, largest first (longest-processing-time order).  The per-mesh pipeline has
+// host-sized stages (the (tile, triangle) pair count, the axis-row hit count, the undecided-node
+// count), so one mesh alone leaves the GPU idle while its host thread waits; several workers fill
+// those gaps with the kernels of other meshes.
+//
+// Reference-rule and h-bounded batches run in three phases:
+//   1. the workers prepare every item -- mesh records and LBVH, the distance tile lists, the whole
+//      sign stage -- each item in its own buffers (scratch names in a per-worker slot namespace, so
+//      repeated batches reuse them);
+//   2. the folds of all items run in ONE persistent kernel (k_tile_fold_multi: CTAs stride over the
+//      (item, tile) work list of the whole batch, one tile volume for all, autotuned on the largest
+//      item), followed by every item's 3-nearest-vertex fallback and combine -- the whole sequence
+//      captured in one CUDA graph and launched once;
+//   3. the fields are copied to the callers' buffers.
+// Unbounded batches keep the per-item pipeline (their search has no tile lists).
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstring>
 #include <mutex>
 #include <numeric>
 #include <thread>
@@ -134,7 +145,8 @@ int autotune_tile(sdfgpu_ctx* ctx, const double origin[3], double h, const int64
 namespace {
 
 int pick_tile(BatchJob& J, sdfgpu_ctx* w, const sdfgpu_batch_item& it) {
-  const int64_t key = size_class(it);
+  // per mode: the unbounded mode tunes warp bricks, the others tiles
+  const int64_t key = size_class(it) * 4 + J.mode;
   {
     std::lock_guard<std::mutex> lk(J.mu);
     auto f = J.parent->tuned.find(key);
@@ -152,6 +164,7 @@ int pick_tile(BatchJob& J, sdfgpu_ctx* w, const sdfgpu_batch_item& it) {
 
 void worker_main(BatchJob& J, sdfgpu_ctx* w) {
   const int64_t n = (int64_t)J.order.size();
+  w->ns.clear();
   for (;;) {
     if (J.stop.load()) return;
     const int64_t k = J.next.fetch_add(1);
@@ -180,6 +193,151 @@ void worker_main(BatchJob& J, sdfgpu_ctx* w) {
   }
 }
 
+// One prepared item of a persistent batch.
+struct Prepared {
+  DistPlan plan;
+  double *d_dist = nullptr, *d_sign = nullptr, *d_conf = nullptr, *d_sdf = nullptr;
+  int64_t ngp = 0;
+};
+
+// Phase 1 of a reference-rule / h-bounded batch: everything but the fold, fallback and combine,
+// for the items assigned to this worker (`mine`, a fixed longest-processing-time assignment, so a
+// repeated batch puts every item in the same worker slot and its buffers are reused as they are).
+void worker_prepare(BatchJob& J, sdfgpu_ctx* w, const std::vector<int64_t>& mine, std::vector<Prepared>& prep) {
+  int slot = 0;
+  for (const int64_t i : mine) {
+    if (J.stop.load()) return;
+    sdfgpu_batch_item& it = J.items[i];
+    Prepared& P = prep[(size_t)i];
+    w->ns = "s" + std::to_string(slot++) + ":";
+    int rc = sdfgpu_set_mesh(w, it.X, it.nnp, it.IEN, it.nel);
+    sdfgpu_stats ms = w->stats;
+    if (rc == 0 && J.autotune) rc = pick_tile(J, w, it);
+    GridP g;
+    if (rc == 0) rc = make_grid(w, it.origin, it.h, it.N, g);
+    if (rc == 0) rc = scratch_t(w, "out_dist", (size_t)g.ngp, &P.d_dist);
+    if (rc == 0) rc = scratch_t(w, "out_sign", (size_t)g.ngp, &P.d_sign);
+    if (rc == 0) rc = scratch_t(w, "out_conf", (size_t)g.ngp, &P.d_conf);
+    if (rc == 0) rc = scratch_t(w, "out_sdf", (size_t)g.ngp, &P.d_sdf);
+    if (rc == 0)
+      rc = run_all(w, g, true, true, J.mode, 0, J.min_rays, J.max_rays, J.conf, J.use_winding, P.d_dist, nullptr,
+                   P.d_sign, P.d_conf, P.d_sdf, &P.plan);
+    P.ngp = g.ngp;
+    std::lock_guard<std::mutex> lk(J.mu);
+    if (rc != 0) {
+      if (J.rc == 0) {
+        J.rc = rc;
+        J.err = "batch item " + std::to_string(i) + ": " + w->err;
+      }
+      J.stop.store(true);
+      return;
+    }
+    sdfgpu_stats s = w->stats;
+    s.ms_mesh = ms.ms_mesh;
+    s.mesh_launches = ms.mesh_launches;
+    add_stats(J.stats, s);
+  }
+}
+
+// Phases 2 and 3 on ctx's stream: one graph with the persistent fold of every item, then each
+// item's fallback and combine; then the copies to the callers' buffers.
+int run_persistent(sdfgpu_ctx* ctx, BatchJob& J, std::vector<Prepared>& prep, int nw, int threads) {
+  cudaStream_t st = ctx->stream;
+  for (int k = 0; k < nw; ++k) {  // everything the workers enqueued is done
+    sdfgpu_ctx* w = ctx->workers[k];
+    SDF_CUDA(ctx, cudaStreamSynchronize(w->stream));
+    SDF_CUDA(ctx, cudaStreamSynchronize(w->sign_stream));
+    SDF_CUDA(ctx, cudaStreamSynchronize(w->bvh_stream));
+  }
+  const int64_t count = (int64_t)prep.size();
+  const size_t sz = fold_args_size();
+  std::vector<unsigned char> args(sz * (size_t)count);
+  std::vector<int64_t> off((size_t)count);
+  int64_t total = 0;
+  for (int64_t i = 0; i < count; ++i) {
+    plan_set_counters(prep[i].plan, ctx->d_counters);
+    std::memcpy(args.data() + sz * (size_t)i, prep[i].plan.fold, sz);
+    off[(size_t)i] = total;
+    total += prep[i].plan.ntiles;
+  }
+  void* d_args;
+  int64_t* d_off;
+  SDF_TRY(scratch(ctx, "batch_args", args.size(), &d_args));
+  SDF_TRY(scratch_t(ctx, "batch_off", (size_t)count, &d_off));
+  SDF_TRY(reset_counters(ctx));
+  SDF_CUDA(ctx, cudaMemcpyAsync(d_args, args.data(), args.size(), cudaMemcpyHostToDevice, st));
+  SDF_CUDA(ctx, cudaMemcpyAsync(d_off, off.data(), sizeof(int64_t) * count, cudaMemcpyHostToDevice, st));
+  int64_t grid = 1;
+  SDF_TRY(dist_fold_multi_grid(ctx, threads, total, &grid));
+  SDF_CUDA(ctx, cudaStreamSynchronize(st));  // the argument arrays are in place before the capture
+
+  // the items' fallbacks and combines after the fold, on the (idle) worker streams side by side
+  std::vector<cudaEvent_t> evs((size_t)nw + 1, nullptr);
+  for (auto& e : evs)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      for (auto& x : evs)
+        if (x) cudaEventDestroy(x);
+      return fail(ctx, SDFGPU_ERR_CUDA, "batch: cudaEventCreate failed");
+    }
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  SDF_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  int rc = dist_fold_multi(ctx, d_args, d_off, (int)count, total, threads, grid, st);
+  if (rc == 0 && cudaEventRecord(evs[(size_t)nw], st) != cudaSuccess) rc = fail(ctx, SDFGPU_ERR_CUDA, "batch fork");
+  for (int k = 0; k < nw && rc == 0; ++k)
+    if (cudaStreamWaitEvent(ctx->workers[k]->stream, evs[(size_t)nw], 0) != cudaSuccess)
+      rc = fail(ctx, SDFGPU_ERR_CUDA, "batch fork");
+  for (int64_t i = 0; i < count && rc == 0; ++i) {
+    const Prepared& P = prep[(size_t)i];
+    cudaStream_t si = ctx->workers[i % nw]->stream;
+    if (P.plan.knn) rc = dist_knn(ctx, P.plan, si, false);
+    if (rc == 0) rc = launch_combine(ctx, P.ngp, P.d_dist, P.d_sign, P.d_sdf, si);
+  }
+  for (int k = 0; k < nw; ++k)  // join every forked stream, also after a failure, to end the capture
+    if (cudaEventRecord(evs[(size_t)k], ctx->workers[k]->stream) == cudaSuccess)
+      cudaStreamWaitEvent(st, evs[(size_t)k], 0);
+  const cudaError_t ce = cudaStreamEndCapture(st, &graph);  // always leave capture mode
+  for (auto& e : evs) cudaEventDestroy(e);
+  if (rc == 0 && ce != cudaSuccess) rc = fail(ctx, SDFGPU_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(ce));
+  if (rc == 0) {
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) rc = fail(ctx, SDFGPU_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  }
+  float ms = 0.f;
+  if (rc == 0 && (cudaEventRecord(ctx->ev[0], st) != cudaSuccess || cudaGraphLaunch(exec, st) != cudaSuccess ||
+                  cudaEventRecord(ctx->ev[1], st) != cudaSuccess))
+    rc = fail(ctx, SDFGPU_ERR_CUDA, "batch graph launch failed");
+  for (int64_t i = 0; i < count && rc == 0; ++i) {
+    const sdfgpu_batch_item& it = J.items[i];
+    const Prepared& P = prep[(size_t)i];
+    const size_t bytes = sizeof(double) * (size_t)P.ngp;
+    cudaError_t e = cudaMemcpyAsync(it.sdf, P.d_sdf, bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && it.dist) e = cudaMemcpyAsync(it.dist, P.d_dist, bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && it.sign) e = cudaMemcpyAsync(it.sign, P.d_sign, bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && it.conf) e = cudaMemcpyAsync(it.conf, P.d_conf, bytes, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) rc = fail(ctx, SDFGPU_ERR_CUDA, std::string("batch copy: ") + cudaGetErrorString(e));
+  }
+  int64_t c[C_NUM] = {};
+  if (rc == 0) {
+    cudaError_t e = cudaMemcpyAsync(c, ctx->d_counters, sizeof(c), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    if (e != cudaSuccess) rc = fail(ctx, SDFGPU_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(e));
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  if (rc != 0) return rc;
+  if (c[C_ERR_STACK]) return fail(ctx, SDFGPU_ERR_CAPACITY, "BVH traversal stack overflow");
+  if (c[C_ERR_CAPACITY]) return fail(ctx, SDFGPU_ERR_CAPACITY, "a per-node candidate buffer overflowed");
+  J.stats.fp64_evals += c[C_FP64];
+  J.stats.candidate_nodes += c[C_CAND_NODES];
+  J.stats.knn_fallback_nodes += c[C_KNN];
+  J.stats.ms_fold += ms;
+  J.stats.ms_distance += ms;
+  J.stats.launches += 1 + count;
+  return 0;
+}
+
 }  // namespace
 }  // namespace sdfgpu
 
@@ -204,6 +362,13 @@ int sdfgpu_autotune(sdfgpu_ctx* ctx, const double origin[3], double h, const int
 int sdfgpu_sdf_batch(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count, int32_t mode, int32_t min_rays,
                      int32_t max_rays, double confidence_threshold, int32_t use_winding_fallback, int32_t streams,
                      int32_t autotune) {
+  return sdfgpu_sdf_batch_ex(ctx, items, count, mode, min_rays, max_rays, confidence_threshold, use_winding_fallback,
+                             streams, autotune, 0);
+}
+
+int sdfgpu_sdf_batch_ex(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count, int32_t mode, int32_t min_rays,
+                        int32_t max_rays, double confidence_threshold, int32_t use_winding_fallback, int32_t streams,
+                        int32_t autotune, int32_t persistent) {
   SDF_TRY(begin_call(ctx));
   if (count < 0 || (count > 0 && !items)) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "items must hold count entries");
   if (streams < 0 || streams > kMaxStreams)
@@ -248,11 +413,36 @@ int sdfgpu_sdf_batch(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count, i
       }
   std::vector<std::thread> threads;
   threads.reserve(nw);
-  for (int k = 0; k < nw; ++k) threads.emplace_back(worker_main, std::ref(J), ctx->workers[k]);
+  if (mode == SDFGPU_MODE_UNBOUNDED || !persistent) {  // per-item pipelines
+    for (int k = 0; k < nw; ++k) threads.emplace_back(worker_main, std::ref(J), ctx->workers[k]);
+    for (auto& t : threads) t.join();
+    ctx->stats = J.stats;
+    if (J.rc != 0) return fail(ctx, J.rc, J.err);
+    return SDFGPU_OK;
+  }
+  // Fixed longest-processing-time assignment of the items to the workers.
+  std::vector<std::vector<int64_t>> mine((size_t)nw);
+  {
+    std::vector<double> load((size_t)nw, 0.0);
+    for (const int64_t i : J.order) {
+      const size_t k = (size_t)(std::min_element(load.begin(), load.end()) - load.begin());
+      mine[k].push_back(i);
+      load[k] += item_work(items[i]);
+    }
+  }
+  std::vector<Prepared> prep((size_t)count);
+  for (int k = 0; k < nw; ++k)
+    threads.emplace_back(worker_prepare, std::ref(J), ctx->workers[k], std::cref(mine[(size_t)k]), std::ref(prep));
   for (auto& t : threads) t.join();
+  if (J.rc != 0) {
+    ctx->stats = J.stats;
+    return fail(ctx, J.rc, J.err);
+  }
+  int tvol = 32;  // the persistent fold's CTA holds the largest tile of the batch
+  for (const Prepared& P : prep) tvol = std::max(tvol, P.plan.threads);
+  const int rc = run_persistent(ctx, J, prep, nw, tvol);
   ctx->stats = J.stats;
-  if (J.rc != 0) return fail(ctx, J.rc, J.err);
-  return SDFGPU_OK;
+  return rc;
 }
 
 }  // extern "C"

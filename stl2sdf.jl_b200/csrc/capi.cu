@@ -19,7 +19,7 @@ int fail(sdfgpu_ctx* ctx, int code, const std::string& msg) {
 }
 
 int scratch(sdfgpu_ctx* ctx, const char* name, size_t bytes, void** out) {
-  DevBuf& b = ctx->bufs[name];
+  DevBuf& b = ctx->ns.empty() ? ctx->bufs[name] : ctx->bufs[ctx->ns + name];
   if (b.cap < bytes) {
     if (b.p) {
       cudaError_t e = cudaFree(b.p);
@@ -233,7 +233,7 @@ int check_mode(sdfgpu_ctx* ctx, int mode, int learned) {
 // Runs the requested stages into device buffers.
 int run_all(sdfgpu_ctx* ctx, const GridP& g, bool want_dist, bool want_sign, int mode, int learned, int min_rays,
             int max_rays, double conf, int use_winding, double* d_dist, double* d_xp, double* d_sign, double* d_conf,
-            double* d_sdf) {
+            double* d_sdf, DistPlan* defer) {
   SDF_TRY(reset_counters(ctx));
   ctx->launches = 0;
   for (int i = 0; i < T_NUM; ++i) SDF_MARK(ctx, i);
@@ -242,26 +242,45 @@ int run_all(sdfgpu_ctx* ctx, const GridP& g, bool want_dist, bool want_sign, int
   // the rest of the sign stage while the distance fold runs.  The join precedes the combine.
   cudaStream_t ss = ctx->sign_stream;
   SignPlan P;
-  if (want_sign) {
-    SDF_CUDA(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
-    SDF_CUDA(ctx, cudaStreamWaitEvent(ss, ctx->ev_fork, 0));
-    SDF_MARK_ON(ctx, T_SIGN0, ss);
-    SDF_TRY(sign_begin(ctx, g, P));
+  bool forked = false;
+  // Every exit, failures included, leaves the context stream ordered after the sign stream and
+  // the LBVH build, so nothing of this call is still running behind the next one.
+  auto join = [&]() {
+    if (forked && cudaEventRecord(ctx->ev_join, ss) == cudaSuccess) cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0);
+    forked = false;
+    cudaStreamWaitEvent(ctx->stream, ctx->ev_bvh, 0);
+  };
+  auto stages = [&]() -> int {
+    if (want_sign) {
+      SDF_CUDA(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
+      SDF_CUDA(ctx, cudaStreamWaitEvent(ss, ctx->ev_fork, 0));
+      forked = true;
+      SDF_MARK_ON(ctx, T_SIGN0, ss);
+      SDF_TRY(sign_begin(ctx, g, P));
+    }
+    if (want_dist) {
+      if (defer)  // a batch runs the fold later, together with other meshes'
+        SDF_TRY(dist_prepare(ctx, g, mode, d_dist, d_xp, *defer));
+      else
+        SDF_TRY(run_distances(ctx, g, mode, learned, d_dist, d_xp));
+    }
+    SDF_MARK(ctx, T_DIST1);
+    if (want_sign) {
+      for (int i = T_ROWS; i <= T_PARITY; ++i) SDF_MARK_ON(ctx, i, ss);
+      // Rays past the 36th are never cast, so every max_rays >= 44 gives the same votes as 44.
+      const int max_eff = max_rays > 44 ? 44 : max_rays;
+      SDF_TRY(sign_finish(ctx, g, P, min_rays, max_eff, conf, use_winding, d_sign, d_conf));
+      SDF_MARK_ON(ctx, T_SIGN1, ss);
+    }
+    join();
+    if (want_dist && want_sign && d_sdf && !defer) SDF_TRY(run_combine(ctx, g, d_dist, d_sign, d_sdf));
+    return 0;
+  };
+  const int rc = stages();
+  if (rc != 0) {
+    join();
+    return rc;
   }
-  if (want_dist) SDF_TRY(run_distances(ctx, g, mode, learned, d_dist, d_xp));
-  SDF_MARK(ctx, T_DIST1);
-  if (want_sign) {
-    for (int i = T_ROWS; i <= T_PARITY; ++i) SDF_MARK_ON(ctx, i, ss);
-    // Rays past the 36th are never cast, so every max_rays >= 44 gives the same votes as 44.
-    const int max_eff = max_rays > 44 ? 44 : max_rays;
-    SDF_TRY(sign_finish(ctx, g, P, min_rays, max_eff, conf, use_winding, d_sign, d_conf));
-    SDF_MARK_ON(ctx, T_SIGN1, ss);
-    SDF_CUDA(ctx, cudaEventRecord(ctx->ev_join, ss));
-    SDF_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
-  }
-  if (want_dist && want_sign && d_sdf) SDF_TRY(run_combine(ctx, g, d_dist, d_sign, d_sdf));
-  // a call ends after the mesh's LBVH build too, whether or not this call used it
-  SDF_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_bvh, 0));
   SDF_TRY(finish_counters(ctx, g));
   auto span = [&](int a, int b, double* out) -> int {
     float ms = 0.f;

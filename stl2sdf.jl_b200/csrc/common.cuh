@@ -113,8 +113,9 @@ struct sdfgpu_ctx {
   cudaEvent_t ev_mesh = nullptr;         // triangle records ready (on the context stream)
   cudaEvent_t ev_bvh = nullptr;          // LBVH of the current mesh complete (on bvh_stream)
   int64_t* h_scalars = nullptr;          // page-locked host slots for sizing reads (see Scalar)
+  std::string ns;                        // prefix of every scratch-buffer name (batch items keep their own)
   std::vector<sdfgpu_ctx*> workers;      // batch workers (batch.cu), created on first use
-  std::map<int64_t, uint32_t> tuned;     // autotuner: size class -> packed tile (batch.cu)
+  std::map<int64_t, uint32_t> tuned;     // autotuner: (size class, mode) -> packed tile or brick (batch.cu)
 };
 
 namespace sdfgpu {
@@ -166,7 +167,7 @@ inline int scratch_t(sdfgpu_ctx* ctx, const char* name, size_t count, T** out) {
 
 template <class T>
 inline T* buf(sdfgpu_ctx* ctx, const char* name) {
-  auto it = ctx->bufs.find(name);
+  auto it = ctx->ns.empty() ? ctx->bufs.find(name) : ctx->bufs.find(ctx->ns + name);
   return it == ctx->bufs.end() ? nullptr : (T*)it->second.p;
 }
 
@@ -201,9 +202,12 @@ int reset_counters(sdfgpu_ctx* ctx);
 int finish_counters(sdfgpu_ctx* ctx, const GridP& g);
 int check_sign_args(sdfgpu_ctx* ctx, int min_rays, int max_rays, double conf);
 int check_mode(sdfgpu_ctx* ctx, int mode, int learned);
+struct DistPlan;
+// All stages of one grid call.  With `defer`, the distance stage stops after its tile lists (its
+// fold, fallback and the combine are left to the caller, described by *defer).
 int run_all(sdfgpu_ctx* ctx, const GridP& g, bool want_dist, bool want_sign, int mode, int learned, int min_rays,
             int max_rays, double conf, int use_winding, double* d_dist, double* d_xp, double* d_sign, double* d_conf,
-            double* d_sdf);
+            double* d_sdf, DistPlan* defer = nullptr);
 
 // Fills GridP from (origin, h, N) and the current mesh frame; validates sizes.
 // k0..k1 (inclusive, k1 >= 0) restricts the call to those z layers of the grid (a z-slab);
@@ -216,6 +220,34 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
                           bool device_ptrs);
 int ensure_ine(sdfgpu_ctx* ctx);
 int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, double* d_dist, double* d_xp);
+
+// The reference-rule / h-bounded distance stage in parts (distance.cu), so a batch can run the folds
+// of many meshes in one launch: dist_prepare builds one mesh's tile lists and fold arguments,
+// dist_fold runs one mesh's fold, dist_knn its 3-nearest-vertex fallback, dist_fold_multi the
+// folds of many prepared meshes together.
+struct DistPlan {
+  alignas(16) unsigned char fold[448];      // the fold kernel's arguments
+  alignas(16) unsigned char knn_args[448];  // the fallback kernel's arguments (when knn)
+  GridP g;
+  int64_t ntiles = 0;
+  int threads = 0;
+  bool knn = false;                         // the fallback runs after the fold
+  uint8_t* band = nullptr;                  // nodes within h of a triangle (NULL: every empty node)
+  const float4* band_v32 = nullptr;
+  const TriRec64* band_rec = nullptr;
+  int64_t nel = 0;
+  double hb = 0.0;
+};
+int dist_prepare(sdfgpu_ctx* ctx, const GridP& g, int mode, double* d_dist, double* d_xp, DistPlan& P);
+int dist_fold(sdfgpu_ctx* ctx, const DistPlan& P);
+int dist_knn(sdfgpu_ctx* ctx, const DistPlan& P, cudaStream_t st, bool wait_bvh);
+int dist_fold_multi_grid(sdfgpu_ctx* ctx, int threads, int64_t total, int64_t* grid);
+int dist_fold_multi(sdfgpu_ctx* ctx, const void* d_args, const int64_t* d_off, int count, int64_t total, int threads,
+                    int64_t grid, cudaStream_t st);
+size_t fold_args_size();
+void plan_set_counters(DistPlan& P, int64_t* counters);
+int launch_combine(sdfgpu_ctx* ctx, int64_t ngp, const double* d_dist, const double* d_sign, double* d_sdf,
+                   cudaStream_t st);
 // The sign stage in two parts on ctx->sign_stream: sign_begin enqueues the axis-row counting and
 // returns without waiting; sign_finish waits for that count and enqueues the rest (lists, parities,
 // vote, adaptive rays, winding).  Between the two the caller can enqueue the distance stage, which

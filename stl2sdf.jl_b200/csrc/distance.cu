@@ -28,6 +28,8 @@
 // the tile; SDFGPU_MODE_UNBOUNDED is a per-node LBVH nearest-triangle search without the clamp.
 #include <cub/cub.cuh>
 
+#include <cstring>
+
 #include "common.cuh"
 #include "fold32.cuh"
 
@@ -163,16 +165,16 @@ struct __align__(16) WarpStage {
 //   the FP32 replay of the reference step (fold32.cuh).  Only a decision inside its error band
 //   runs the FP64 reference step (exact64.cuh); the FP64 value of the final winner is recomputed
 //   once, so the output has the reference arithmetic's bits.
-__global__ void __launch_bounds__(256) k_tile_fold(FoldArgs A) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void fold_tile(const FoldArgs& A, int64_t tile, unsigned char* smem_raw) {
   WarpStage& S = reinterpret_cast<WarpStage*>(smem_raw)[threadIdx.x >> 5];
   const unsigned lane = threadIdx.x & 31;
   const GridP& g = A.g;
-  const int64_t tile = blockIdx.x;
   const int64_t tx = tile % g.nt[0], ty = (tile / g.nt[0]) % g.nt[1], tz = tile / (g.nt[0] * g.nt[1]);
   const int lx = threadIdx.x % g.t[0], ly = (threadIdx.x / g.t[0]) % g.t[1], lz = threadIdx.x / (g.t[0] * g.t[1]);
   const int64_t i = tx * g.t[0] + lx, j = ty * g.t[1] + ly, k = tz * g.t[2] + lz;
-  const bool valid = i <= g.N[0] && j <= g.N[1] && k <= g.N[2];
+  // lz < t[2]: a CTA larger than the tile (a multi-mesh launch sized for its largest tile) has threads
+  // past the tile, which only take part in the warp-wide steps
+  const bool valid = lz < g.t[2] && i <= g.N[0] && j <= g.N[1] && k <= g.N[2];
   const int64_t lin = i + g.n[0] * (j + g.n[1] * k);
   const d3 p = gnode(g, i, j, k);
   const d3 t0 = gnode(g, tx * g.t[0], ty * g.t[1], tz * g.t[2]);
@@ -299,6 +301,37 @@ __global__ void __launch_bounds__(256) k_tile_fold(FoldArgs A) {
   if (lane == 0) {
     if (fp64) count_add(A.counters, C_FP64, fp64);
     if (cand) count_add(A.counters, C_CAND_NODES, cand);
+  }
+}
+
+
+__global__ void __launch_bounds__(256) k_tile_fold(FoldArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  fold_tile(A, blockIdx.x, smem_raw);
+}
+
+// The fold of many meshes in one persistent launch: work item w (0 <= w < total) is tile
+// w - off[m] of mesh m, off[] the exclusive prefix of the meshes' tile counts; CTAs stride over the
+// items.  Each mesh keeps its own tile shape; the CTA holds the largest tile of the batch.
+__global__ void __launch_bounds__(256) k_tile_fold_multi(const FoldArgs* __restrict__ args,
+                                                         const int64_t* __restrict__ off, int nmesh, int64_t total) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ __align__(16) unsigned char sA_raw[sizeof(FoldArgs)];
+  __shared__ int s_mesh;
+  FoldArgs& sA = *reinterpret_cast<FoldArgs*>(sA_raw);
+  for (int64_t w = blockIdx.x; w < total; w += gridDim.x) {
+    if (threadIdx.x == 0) {
+      int lo = 0, hi = nmesh - 1;  // the last mesh whose first item is <= w
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= w) lo = mid; else hi = mid - 1;
+      }
+      s_mesh = lo;
+      sA = args[lo];
+    }
+    __syncthreads();
+    fold_tile(sA, w - off[s_mesh], smem_raw);
+    __syncthreads();  // sA and s_mesh are rewritten for the next item
   }
 }
 
@@ -741,6 +774,31 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
     return 0;
   }
 
+  DistPlan P;
+  SDF_TRY(dist_prepare(ctx, g, mode, d_dist, d_xp, P));
+  SDF_MARK(ctx, T_TILES);
+  SDF_TRY(dist_fold(ctx, P));
+  SDF_MARK(ctx, T_FOLD);
+  if (P.knn) SDF_TRY(dist_knn(ctx, P, st, true));
+  return 0;
+}
+
+// Tile lists of the reference rule (or the h-bounded exact mode) and the fold's arguments; when the
+// mesh needs the 3-nearest-vertex fallback, its incidence lists, band flags and arguments too.
+int dist_prepare(sdfgpu_ctx* ctx, const GridP& g, int mode, double* d_dist, double* d_xp, DistPlan& Pl) {
+  static_assert(sizeof(FoldArgs) <= sizeof(Pl.fold), "DistPlan::fold too small");
+  static_assert(sizeof(KnnArgs) <= sizeof(Pl.knn_args), "DistPlan::knn_args too small");
+  cudaStream_t st = ctx->stream;
+  const MeshDev& M = ctx->mesh;
+  const int64_t nel = M.nel;
+  TriRec64* rec = buf<TriRec64>(ctx, "rec");
+  double4* cent = buf<double4>(ctx, "cent64");
+  float4* v32 = buf<float4>(ctx, "v32");
+  float4* c32 = buf<float4>(ctx, "c32");
+  const float E = (float)g.E;
+  const float eD_abs = 4.0e-6f * E;
+  const float eD_rel = 4.0e-6f;
+  const float pad = 2.0e-6f * E;
   const double sr = 2.5 * g.h;
   const double R = mode == SDFGPU_MODE_REF_RULE ? sr * (1.0 + 1e-9) + 1e-6 * g.E : g.h * (1.0 + 1e-9) + 1e-6 * g.E;
   int32_t *tri_cnt, *tri_off, *tile_cnt, *tile_off, *vals, *vals2;
@@ -800,16 +858,12 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
   A.xp = d_xp;
   A.status = status;
   A.counters = ctx->d_counters;
-  const int threads = g.t[0] * g.t[1] * g.t[2];
   if (g.ntiles > 0x7fffffffLL) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "grid has too many tiles");
-  SDF_MARK(ctx, T_TILES);
-  const size_t smem = sizeof(WarpStage) * (size_t)(threads / 32);
-  if (smem > 48 * 1024)  // tiles of more than 5 warps stage more than the default 48 KB
-    SDF_CUDA(ctx, cudaFuncSetAttribute(k_tile_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_tile_fold<<<(unsigned)g.ntiles, threads, smem, st>>>(A);
-  SDF_KERNEL(ctx);
-  SDF_MARK(ctx, T_FOLD);
-
+  std::memcpy(Pl.fold, &A, sizeof(A));
+  Pl.g = g;
+  Pl.ntiles = g.ntiles;
+  Pl.threads = g.t[0] * g.t[1] * g.t[2];
+  Pl.knn = false;
   if (mode == SDFGPU_MODE_REF_RULE) {
     // Can a node with an empty candidate set still have a triangle within h?  Only when some
     // triangle reaches farther than 1.5h from its centroid (|c - p| <= d + rho <= h + rho).
@@ -817,19 +871,13 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
     if (big_tris || d_xp) {
       SDF_TRY(ensure_ine(ctx));
       uint8_t* band = nullptr;
-      if (!d_xp) {
-        SDF_TRY(scratch_t(ctx, "band", (size_t)g.ngp, &band));
-        SDF_CUDA(ctx, cudaMemsetAsync(band, 0, (size_t)g.ngp, st));
-        const double hb = g.h * (1.0 + 1e-9) + (double)eD_abs + 2e-6 * g.E;
-        k_band<<<grid_for(nel, 128), 128, 0, st>>>(v32, rec, nel, g, hb, (float)(hb * hb), band);
-        SDF_KERNEL(ctx);
-      }
+      if (!d_xp) SDF_TRY(scratch_t(ctx, "band", (size_t)g.ngp, &band));
       KnnArgs K;
       K.g = g;
       K.status = status;
       K.band = band;
-      K.nodes = nodes;
-      K.leaf_prim = leaf_prim;
+      K.nodes = buf<BNode>(ctx, "nodes");
+      K.leaf_prim = buf<int32_t>(ctx, "leaf_prim");
       K.tri_idx = nullptr;
       K.IEN = buf<int64_t>(ctx, "IEN64");
       K.X = buf<double>(ctx, "X64");
@@ -841,12 +889,87 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
       K.dist = d_dist;
       K.xp = d_xp;
       K.counters = ctx->d_counters;
-      SDF_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_bvh, 0));  // the fallback walks the LBVH
-      k_knn_fallback<<<grid_for(g.ngp, 128, 148 * 16), 128, 0, st>>>(K);
-      SDF_KERNEL(ctx);
+      std::memcpy(Pl.knn_args, &K, sizeof(K));
+      Pl.knn = true;
+      Pl.band = band;
+      Pl.band_v32 = v32;
+      Pl.band_rec = rec;
+      Pl.nel = nel;
+      Pl.hb = g.h * (1.0 + 1e-9) + (double)eD_abs + 2e-6 * g.E;
     }
   }
   return 0;
+}
+
+// The fold of one mesh on the context stream (one CTA per tile).
+int dist_fold(sdfgpu_ctx* ctx, const DistPlan& Pl) {
+  FoldArgs A;
+  std::memcpy(&A, Pl.fold, sizeof(A));
+  const size_t smem = sizeof(WarpStage) * (size_t)(Pl.threads / 32);
+  if (smem > 48 * 1024)  // tiles of more than 5 warps stage more than the default 48 KB
+    SDF_CUDA(ctx, cudaFuncSetAttribute(k_tile_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_tile_fold<<<(unsigned)Pl.ntiles, Pl.threads, smem, ctx->stream>>>(A);
+  SDF_KERNEL(ctx);
+  return 0;
+}
+
+// The 3-nearest-vertex fallback after the fold, on stream st: launches only (no allocation, no host
+// wait), so it can be captured in a graph.  wait_bvh: order st after the LBVH build first.
+int dist_knn(sdfgpu_ctx* ctx, const DistPlan& Pl, cudaStream_t st, bool wait_bvh) {
+  const GridP& g = Pl.g;
+  if (Pl.band) {
+    SDF_CUDA(ctx, cudaMemsetAsync(Pl.band, 0, (size_t)g.ngp, st));
+    k_band<<<grid_for(Pl.nel, 128), 128, 0, st>>>(Pl.band_v32, Pl.band_rec, Pl.nel, g, Pl.hb, (float)(Pl.hb * Pl.hb),
+                                                   Pl.band);
+    SDF_KERNEL(ctx);
+  }
+  if (wait_bvh) SDF_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_bvh, 0));  // the fallback walks the LBVH
+  KnnArgs K;
+  std::memcpy(&K, Pl.knn_args, sizeof(K));
+  k_knn_fallback<<<grid_for(g.ngp, 128, 148 * 16), 128, 0, st>>>(K);
+  SDF_KERNEL(ctx);
+  return 0;
+}
+
+// The folds of several meshes (plans prepared by dist_prepare on their own contexts, all with the
+// same tile volume) in one persistent launch on stream st.  d_args / d_off: device copies of the
+// plans' fold arguments and of the exclusive prefix of their tile counts, already uploaded.
+// Resident CTAs of the multi-mesh fold (all SMs at full occupancy, at most one per work item); also
+// raises the kernel's shared-memory limit when needed.  Call before a stream capture.
+int dist_fold_multi_grid(sdfgpu_ctx* ctx, int threads, int64_t total, int64_t* grid) {
+  const size_t smem = sizeof(WarpStage) * (size_t)(threads / 32);
+  if (smem > 48 * 1024)
+    SDF_CUDA(ctx, cudaFuncSetAttribute(k_tile_fold_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0, sms = 148;
+  SDF_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_fold_multi, threads, smem));
+  SDF_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  *grid = std::max<int64_t>(1, std::min<int64_t>(total, (int64_t)sms * std::max(per_sm, 1)));
+  return 0;
+}
+
+int dist_fold_multi(sdfgpu_ctx* ctx, const void* d_args, const int64_t* d_off, int count, int64_t total, int threads,
+                    int64_t grid, cudaStream_t st) {
+  if (count < 1 || total < 1) return 0;
+  const size_t smem = sizeof(WarpStage) * (size_t)(threads / 32);
+  k_tile_fold_multi<<<(unsigned)grid, threads, smem, st>>>((const FoldArgs*)d_args, d_off, count, total);
+  SDF_KERNEL(ctx);
+  return 0;
+}
+
+size_t fold_args_size() { return sizeof(FoldArgs); }
+
+// Points a plan's kernels at another counter array (a batch sums its folds' counters in one place).
+void plan_set_counters(DistPlan& Pl, int64_t* counters) {
+  FoldArgs A;
+  std::memcpy(&A, Pl.fold, sizeof(A));
+  A.counters = counters;
+  std::memcpy(Pl.fold, &A, sizeof(A));
+  if (Pl.knn) {
+    KnnArgs K;
+    std::memcpy(&K, Pl.knn_args, sizeof(K));
+    K.counters = counters;
+    std::memcpy(Pl.knn_args, &K, sizeof(K));
+  }
 }
 
 }  // namespace sdfgpu

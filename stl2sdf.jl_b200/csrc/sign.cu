@@ -727,7 +727,12 @@ int sign_finish(sdfgpu_ctx* ctx, const GridP& g, SignPlan& P, int min_rays, int 
 
 // sdf = dist .* sign (stl_to_sdf.jl:119) on the context stream.
 int run_combine(sdfgpu_ctx* ctx, const GridP& g, const double* d_dist, const double* d_sign, double* d_sdf) {
-  k_combine<<<grid_for(g.ngp, 256, 148 * 16), 256, 0, ctx->stream>>>(g.ngp, d_dist, d_sign, d_sdf);
+  return launch_combine(ctx, g.ngp, d_dist, d_sign, d_sdf, ctx->stream);
+}
+
+int launch_combine(sdfgpu_ctx* ctx, int64_t ngp, const double* d_dist, const double* d_sign, double* d_sdf,
+                   cudaStream_t st) {
+  k_combine<<<grid_for(ngp, 256, 148 * 16), 256, 0, st>>>(ngp, d_dist, d_sign, d_sdf);
   SDF_KERNEL(ctx);
   return 0;
 }

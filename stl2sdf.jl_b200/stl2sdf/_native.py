@@ -104,6 +104,9 @@ SIGNATURES = {
     "sdfgpu_sdf_batch": ([ctypes.c_void_p, ctypes.POINTER(BatchItem), ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
                           ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32],
                          ctypes.c_int),
+    "sdfgpu_sdf_batch_ex": ([ctypes.c_void_p, ctypes.POINTER(BatchItem), ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
+                             ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                             ctypes.c_int32], ctypes.c_int),
     "sdfgpu_autotune": ([ctypes.c_void_p, _dp, ctypes.c_double, _i64p, ctypes.c_int32,
                          ctypes.POINTER(ctypes.c_int32), _dp], ctypes.c_int),
     "sdfgpu_set_brick": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
@@ -285,7 +288,7 @@ class Context:
                                                  ctypes.c_void_p(conf_ptr or None)))
 
     def sdf_batch(self, meshes, mode=MODE_REF_RULE, min_rays=6, max_rays=30, confidence_threshold=0.6,
-                  use_winding_fallback=True, streams=8, autotune=True, want_parts=False, out=None):
+                  use_winding_fallback=True, streams=8, autotune=True, want_parts=False, out=None, persistent=False):
         """SDFs of many meshes, each on its own grid: meshes = [(X, IEN, origin, h, N), ...].
         Returns one sdf array per mesh (with want_parts, (sdf, dist, sign, conf) per mesh).  `out`
         may supply the sdf arrays (contiguous float64, prod(N+1) each), e.g. views of page-locked
@@ -313,9 +316,9 @@ class Context:
             it.h = float(h)
             it.N[:] = [int(v) for v in N]
             it.sdf, it.dist, it.sign, it.conf = [(_d(a) if a is not None else None) for a in out_k]
-        self._check(lib().sdfgpu_sdf_batch(self._p, items, len(meshes), int(mode), int(min_rays), int(max_rays),
-                                           float(confidence_threshold), int(bool(use_winding_fallback)),
-                                           int(streams), int(bool(autotune))))
+        self._check(lib().sdfgpu_sdf_batch_ex(self._p, items, len(meshes), int(mode), int(min_rays), int(max_rays),
+                                              float(confidence_threshold), int(bool(use_winding_fallback)),
+                                              int(streams), int(bool(autotune)), int(bool(persistent))))
         return [tuple(o) if want_parts else o[0] for o in outs]
 
     def autotune(self, origin, h, N, mode=MODE_REF_RULE):

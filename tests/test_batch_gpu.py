@@ -95,3 +95,33 @@ def test_batch_reports_failing_item(gpu_ctx, small_batch):
         gpu_ctx.sdf_batch(bad, streams=2)
     assert "batch item 1" in str(e.value)
     assert gpu_ctx.sdf_batch([], streams=2) == []
+
+
+def _coarse_sphere_item():
+    """80 large triangles on a fine grid: triangles reach farther than 1.5 cells from their
+    centroids, so the 3-nearest-vertex fallback runs (inside the batch's graph)."""
+    from stl2sdf import DataImport, _native, synthetic
+
+    X, IEN = DataImport.roundtrip_float32(*synthetic.icosphere(1, jitter=0.01, seed=4))
+    o, _, N, h, _ = _native.grid_setup(X.min(0), X.max(0), 48 - 7, 3)
+    return (X, IEN, o, h, N)
+
+
+@pytest.mark.parametrize("persistent", [False, True])
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_batch_modes_equal_single_calls(gpu_ctx, small_batch, mode, persistent):
+    """Both batch forms (per-item pipelines; prepared items with one persistent fold launch in a
+    CUDA graph) give every item exactly its single-call result, twice in a row."""
+    items = list(small_batch[:5]) + [_coarse_sphere_item()]
+    got = gpu_ctx.sdf_batch(items, mode=mode, streams=3, autotune=(mode != 1), want_parts=True, persistent=persistent)
+    again = gpu_ctx.sdf_batch(items, mode=mode, streams=3, autotune=(mode != 1), persistent=persistent)
+    for a, parts in zip(again, got):
+        assert np.array_equal(a, parts[0])
+    st = gpu_ctx.stats()
+    if mode == 0:
+        assert st["knn_fallback_nodes"] > 0  # the coarse sphere took the fallback
+    for (X, IEN, o, h, N), parts in zip(items, got):
+        gpu_ctx.set_mesh(X, IEN)
+        want = gpu_ctx.sdf(o, h, N, mode=mode, want_parts=True)
+        for a, b in zip(parts, want):
+            assert np.array_equal(a, b)
