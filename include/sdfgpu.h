@@ -17,6 +17,12 @@
  *       src/MeshGrid/Grid.jl:9                             -> sdfgpu_grid_setup
  *   noninteractive_sdf_grid_setup(mesh, B)
  *       src/MeshGrid/Grid_setup.jl:104                     -> sdfgpu_grid_from_cell_size
+ *   remove_sdf_artifacts!(sdf, grid; threshold, min_component_ratio)
+ *       src/SignedDistances/SdfArtifactRemoval.jl:134      -> sdfgpu_remove_artifacts
+ *   analyze_sdf_components(sdf, grid; threshold)
+ *       src/SignedDistances/SdfArtifactRemoval.jl:259      -> sdfgpu_sdf_components
+ *   RBFs_smoothing(dist, grid, is_interpolation, smooth, threshold)
+ *       src/SdfSmoothing/RBFs4Smoothing.jl:275              -> sdfgpu_rbf_smoothing
  *
  * Conventions
  *   - Grid nodes are implicit: node (i, j, k), 0 <= i <= N[0] etc., sits at
