@@ -168,7 +168,7 @@ def distance_variants(ctx, X, IEN, g, reps=3, work=None, peak_tflops=None):
     out["learned_unbounded"].update({"certified_fraction": st["certified_nodes"] / g["ngp"],
                                      "fallback_nodes": st["unbounded_fallbacks"], "train_s": train_s,
                                      "train_loss": loss, "train_grid": "64 nodes on the long axis, 1500 Adam steps",
-                                     "margin": "r = (dhat (1 + 0.1) + 1 coarse spacing) s",
+                                     "margin": "r = (dhat (1 + 0.2) + 2 coarse spacings) s",
                                      "bvh_visits_per_node": st["bvh_visits"] / g["ngp"]})
     out["learned_vs_plain_unbounded"] = out["plain_unbounded"]["ms"] / out["learned_unbounded"]["ms"]
     if work is not None and peak_tflops:

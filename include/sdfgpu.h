@@ -260,7 +260,7 @@ int sdfgpu_train_radius(sdfgpu_ctx* ctx, int32_t coarse_n, int32_t steps, int32_
  * product 32) whose nearest triangles one warp searches together.  Default 4 x 2 x 4. */
 int sdfgpu_set_brick(sdfgpu_ctx* ctx, const int32_t brick[3]);
 /* Margin of the learned radius: r = (dhat (1 + alpha) + beta * coarse spacing / s) * s, where dhat is
- * the network's normalised distance and s its normalisation scale.  Defaults alpha = 0.1, beta = 1.
+ * the network's normalised distance and s its normalisation scale.  Defaults alpha = 0.2, beta = 2.
  * A smaller margin prunes more and certifies fewer nodes; results never change. */
 int sdfgpu_set_radius_margin(sdfgpu_ctx* ctx, float alpha, float beta);
 /* Number of FP32 parameters of the radius network (layout: W1 64x32, b1, W2 64x64, b2, W3 64x64,

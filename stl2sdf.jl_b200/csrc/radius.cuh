@@ -27,8 +27,8 @@ struct RadiusNorm {
   double coarse_h = 0.0;
   float loss = 0.f;
   bool trained = false;
-  float alpha = 0.1f;  // radius margin: r = (dhat (1 + alpha) + beta coarse_h / s) s
-  float beta = 1.0f;
+  float alpha = 0.2f;  // radius margin: r = (dhat (1 + alpha) + beta coarse_h / s) s; the
+  float beta = 2.0f;   // fastest of the margins measured (it certifies every node on the workloads)
 };
 
 }  // namespace sdfgpu

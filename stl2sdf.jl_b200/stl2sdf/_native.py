@@ -336,7 +336,7 @@ class Context:
         self._check(lib().sdfgpu_set_brick(self._p, b))
 
     # ---- learned search radius ----
-    def set_radius_margin(self, alpha=0.1, beta=1.0):
+    def set_radius_margin(self, alpha=0.2, beta=2.0):
         """r = (dhat (1 + alpha) + beta * coarse spacing / s) * s."""
         self._check(lib().sdfgpu_set_radius_margin(self._p, float(alpha), float(beta)))
 

@@ -154,3 +154,21 @@ def test_unjittered_sphere_distance_bound():
     r = np.linalg.norm(P, axis=1)
     # inscribed polyhedron: true sphere distance minus the faceting sagitta <= d <= sphere distance + sagitta
     assert np.all(np.abs(d - np.abs(r - 1.0)) < 0.02)
+
+
+def test_work_model_counts_single_triangle():
+    """The roofline's work counts on one triangle (0,0,0)-(1,0,0)-(0,1,0), grid nodes at
+    (0.25|0.75, 0.25|0.75, 0.3|0.8) with h = 0.5, worked out by hand:
+    D*(p) = triangles whose box lies within min(d_true, h) of p; D*_u with d_true alone; row hits =
+    triangles whose box meets the grid line through p along x, y, z."""
+    X = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0]])
+    IEN = np.array([[1, 2, 3]])
+    o, h, N = np.array([0.25, 0.25, 0.3]), 0.5, np.array([1, 1, 1])
+    nodes = np.array([0, 3, 4], dtype=np.int64)  # (0.25,0.25,0.3), (0.75,0.75,0.3), (0.25,0.25,0.8)
+    c = oracle.work_model(X, IEN, o, h, N, nodes)
+    # d_true: 0.3 (face), sqrt(2 * 0.25^2 + 0.3^2) = 0.464 (hypotenuse), 0.8 (> h)
+    assert c["nD"].tolist() == [1, 1, 0]
+    assert c["nD_unb"].tolist() == [1, 1, 1]
+    # only the z line through (x, y) inside the box meets it (z = 0.3 / 0.8 is outside [0, 0])
+    assert c["nrow"].tolist() == [[0, 0, 1], [0, 0, 1], [0, 0, 1]]
+    assert np.all(c["rays"] >= 6)
