@@ -78,3 +78,22 @@ def test_learned_radius_is_exact_and_certifies(gpu_ctx, torus_mesh):
     nodes = np.sort(np.random.default_rng(5).choice(g["ngp"], 2000, replace=False))
     ref, _, _ = oracle.distances(X, IEN, g["origin"], g["h"], g["N"], mode=2, nodes=nodes)
     assert np.array_equal(learned[nodes], ref)
+
+
+def test_tight_margin_falls_back_and_stays_exact(gpu_ctx, torus_mesh):
+    """With no margin about half the nodes are not certified by their bounded search and search
+    again; results still equal the plain unbounded search bit for bit."""
+    X, IEN = torus_mesh
+    g = grid_of(X, n_nodes_long_axis=64)
+    gpu_ctx.set_mesh(X, IEN)
+    gpu_ctx.train_radius(coarse_n=48, steps=600, batch=4096)
+    plain, _ = gpu_ctx.distances(g["origin"], g["h"], g["N"], 2)
+    try:
+        gpu_ctx.set_radius_margin(0.0, 0.0)
+        learned, _ = gpu_ctx.distances(g["origin"], g["h"], g["N"], 2, learned=True)
+        st = gpu_ctx.stats()
+    finally:
+        gpu_ctx.set_radius_margin()
+    assert np.array_equal(plain, learned)
+    assert st["unbounded_fallbacks"] > 0.1 * g["ngp"]
+    assert st["certified_nodes"] + st["unbounded_fallbacks"] == g["ngp"]
