@@ -201,8 +201,12 @@ def run_reference(args, rank, world):
         t0 = time.perf_counter()
         oracle.distances(X, IEN, g["origin"], g["h"], g["N"], mode=0, nodes=nodes, nthreads=nthreads)
         oracle.signs(X, IEN, g["origin"], g["h"], g["N"], nodes=nodes, nthreads=nthreads)
+        dt = time.perf_counter() - t0
         if step >= args.warmup:
-            times.append(time.perf_counter() - t0)
+            times.append(dt)
+        if step == 0:  # size the per-step sample so the whole run takes about 90 s
+            per_step = 90.0 / (args.warmup + args.steps)
+            sample = int(min(sample, max(256, sample / dt * per_step)))
     total = sum(times)
     value = sample * len(times) / total
     line = {
@@ -210,6 +214,7 @@ def run_reference(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "description": desc, "ngp": g["ngp"], "nel": int(IEN.shape[0]),
+                   "N": [int(v) for v in g["N"]], "mode": "ref-rule",
                    "step": f"distance+sign of {sample} seeded grid nodes"},
         "cpu_baseline": {"value": value, "unit": "nodes/s", "cores": nthreads, "kind": "port",
                          "sample": f"{sample} seeded grid nodes per step, distance+sign"},
