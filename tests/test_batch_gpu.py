@@ -125,3 +125,30 @@ def test_batch_modes_equal_single_calls(gpu_ctx, small_batch, mode, persistent):
         want = gpu_ctx.sdf(o, h, N, mode=mode, want_parts=True)
         for a, b in zip(parts, want):
             assert np.array_equal(a, b)
+
+
+def test_workload_batch_items_match_oracle(gpu_ctx):
+    """Workload 4's own recipe (256 meshes, seed 3, grids of 32-160 nodes): the largest icosphere,
+    the largest blob mesh and the coarsest blob mesh (big triangles on a fine grid: the
+    nearest-vertex fallback) through the batch, in both forms, against the oracle on 1,500 seeded
+    nodes each."""
+    from stl2sdf import DataImport, _native, synthetic
+
+    recipes = synthetic.uneven_batch(256, seed=3)
+    ico = [r for r in recipes if r["kind"] == "icosphere"]
+    blob = [r for r in recipes if r["kind"] == "blobs"]
+    picks = [max(ico, key=lambda r: (r["level"], r["K"])), max(blob, key=lambda r: (r["cells"], r["K"])),
+             min(blob, key=lambda r: (r["cells"], -r["K"]))]
+    items = []
+    for r in picks:
+        X, IEN = DataImport.roundtrip_float32(*synthetic.batch_mesh(r))
+        o, _, N, h, _ = _native.grid_setup(X.min(0), X.max(0), r["K"] - 7, 3)
+        items.append((X, IEN, o, h, N))
+    for persistent in (False, True):
+        got = gpu_ctx.sdf_batch(items, streams=3, autotune=True, want_parts=True, persistent=persistent)
+        for (X, IEN, o, h, N), (sdf, dist, sign, conf) in zip(items, got):
+            nodes = sample_nodes(sdf.shape[0], 1500, seed=23)
+            d_ref, _, _ = oracle.distances(X, IEN, o, h, N, mode=0, nodes=nodes)
+            r = oracle.signs(X, IEN, o, h, N, nodes=nodes)
+            assert np.array_equal(dist[nodes], d_ref)
+            assert np.array_equal(sign[nodes], r["sign"]) and np.array_equal(conf[nodes], r["conf"])
