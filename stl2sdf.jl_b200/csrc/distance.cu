@@ -242,12 +242,21 @@ __device__ __forceinline__ void fold_tile(const FoldArgs& A, int64_t tile, unsig
       }
     }
     while (__any_sync(0xffffffffu, bits != 0)) {
-      if (bits) {
-        const int q = __ffs(bits) - 1;
+      // each lane skips, in ascending order, the entries the running minimum has since excluded, so
+      // a warp iteration runs one step on every lane that still has a live entry
+      int q = -1;
+      while (bits) {
+        const int qq = __ffs(bits) - 1;
         bits &= bits - 1;
+        const float lim = m32 + em + cand_err(S.c[qq], plen);
+        if (S.D2[qq][lane] <= lim * lim) {
+          q = qq;
+          break;
+        }
+      }
+      if (q >= 0) {
         const Cand32& c = S.c[q];
-        const float lim = m32 + em + cand_err(c, plen);
-        if (S.D2[q][lane] <= lim * lim) {
+        {
           float val, err;
           int feat;
           const int act = step32(pl, plen, c, m32, em, ref, win_gid, val, feat, err);
