@@ -27,6 +27,7 @@
 // SDFGPU_MODE_EXACT uses the same tiles with lists of the triangles whose box lies within h of
 // the tile; SDFGPU_MODE_UNBOUNDED is a per-node LBVH nearest-triangle search without the clamp.
 #include <cub/cub.cuh>
+#include <cuda_fp16.h>
 
 #include <cstring>
 
@@ -129,6 +130,7 @@ struct FoldArgs {
   int mode;
   const int32_t* tile_off;
   const int32_t* tile_cnt;
+  const int32_t* order;  // tiles by descending list length: work item w folds tile order[w]
   const int32_t* vals;
   const TriRec64* rec;
   const double4* cent;
@@ -146,13 +148,16 @@ struct FoldArgs {
 };
 
 // Per-warp shared staging of 32 list entries in the tile's local frame (origin = the tile's first
-// node): the candidate for the FP32 step, its centroid and box, and per (entry, lane) the FP32
-// point-triangle distance that survived phase A.
+// node): the candidate for the FP32 step, its centroid and box, and per (entry, lane) the squared
+// FP32 point-triangle distance that survived phase A, in units of h^2 and rounded down to FP16.
+// Rounding is monotone, so rd16(fl(D2 / h^2)) <= fl(fl(lim^2) / h^2) whenever D2 <= fl(lim^2): phase
+// B's recheck against the running minimum passes every entry its FP32 form would pass (at worst a
+// few more, which the step then leaves unchanged), at half the shared memory, which buys occupancy.
 struct __align__(16) WarpStage {
   Cand32 c[32];
   float4 cc[32];          // centroid - origin; .w = |centroid - origin|
   float4 lo[32], hi[32];  // box of the triangle in the local frame
-  float D2[32][32];       // [entry][lane]: squared FP32 point-triangle distance
+  __half D2[32][32];      // [entry][lane]: rd16(squared FP32 point-triangle distance / h^2)
 };
 
 // One CTA per tile, one lane per node.  The tile's ascending triangle list is consumed 32 entries
@@ -165,7 +170,8 @@ struct __align__(16) WarpStage {
 //   the FP32 replay of the reference step (fold32.cuh).  Only a decision inside its error band
 //   runs the FP64 reference step (exact64.cuh); the FP64 value of the final winner is recomputed
 //   once, so the output has the reference arithmetic's bits.
-__device__ __forceinline__ void fold_tile(const FoldArgs& A, int64_t tile, unsigned char* smem_raw) {
+__device__ __forceinline__ void fold_tile(const FoldArgs& A, int64_t item, unsigned char* smem_raw) {
+  const int64_t tile = A.order[item];
   WarpStage& S = reinterpret_cast<WarpStage*>(smem_raw)[threadIdx.x >> 5];
   const unsigned lane = threadIdx.x & 31;
   const GridP& g = A.g;
@@ -181,6 +187,7 @@ __device__ __forceinline__ void fold_tile(const FoldArgs& A, int64_t tile, unsig
   const float3 pl = make_float3((float)(p.x - t0.x), (float)(p.y - t0.y), (float)(p.z - t0.z));
   const float plen = len3(pl);
   const float sr = (float)(2.5 * g.h);
+  const float ih2 = fminf((float)(1.0 / (g.h * g.h)), 1.0e30f);  // finite, so 0 * ih2 is 0
   const int32_t start = A.tile_off[tile], end = start + A.tile_cnt[tile];
   const bool ref = A.mode == SDFGPU_MODE_REF_RULE;
   // running minimum: FP32 estimate m32 (error em), exact m64 when m64_ok, else the winner to
@@ -237,7 +244,7 @@ __device__ __forceinline__ void fold_tile(const FoldArgs& A, int64_t tile, unsig
         const float D2 = cand_d2(pl, c);
         if (D2 <= lim2) {
           bits |= 1u << q;
-          S.D2[q][lane] = D2;
+          S.D2[q][lane] = __float2half_rd(D2 * ih2);
         }
       }
     }
@@ -249,7 +256,7 @@ __device__ __forceinline__ void fold_tile(const FoldArgs& A, int64_t tile, unsig
         const int qq = __ffs(bits) - 1;
         bits &= bits - 1;
         const float lim = m32 + em + cand_err(S.c[qq], plen);
-        if (S.D2[qq][lane] <= lim * lim) {
+        if (__half2float(S.D2[qq][lane]) <= lim * lim * ih2) {
           q = qq;
           break;
         }
@@ -341,6 +348,15 @@ __global__ void __launch_bounds__(256) k_tile_fold_multi(const FoldArgs* __restr
     __syncthreads();
     fold_tile(sA, w - off[s_mesh], smem_raw);
     __syncthreads();  // sA and s_mesh are rewritten for the next item
+  }
+}
+
+// Sort keys of the tile order: list length saturated to 16 bits, and the tile index.
+__global__ void k_tile_keys(const int32_t* __restrict__ cnt, int64_t n, uint16_t* __restrict__ key,
+                            int32_t* __restrict__ idx) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+    key[q] = (uint16_t)min(cnt[q], 65535);
+    idx[q] = (int32_t)q;
   }
 }
 
@@ -846,12 +862,32 @@ int dist_prepare(sdfgpu_ctx* ctx, const GridP& g, int mode, double* d_dist, doub
     SDF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys2, vals, vals2, total, 0, bits, st));
   }
   SDF_TRY(cub_scan_i32(ctx, tile_cnt, tile_off, g.ntiles + 1));
+  // Longest lists first: the CTAs of the heaviest tiles start in the first wave and the light ones
+  // fill the last, which shortens the tail of the launch (any order gives the same results).
+  int32_t *ord_in, *order;
+  uint16_t *tkey, *tkey2;
+  SDF_TRY(scratch_t(ctx, "tile_ord_in", (size_t)g.ntiles, &ord_in));
+  SDF_TRY(scratch_t(ctx, "tile_order", (size_t)g.ntiles, &order));
+  SDF_TRY(scratch_t(ctx, "tile_key", (size_t)g.ntiles, &tkey));
+  SDF_TRY(scratch_t(ctx, "tile_key2", (size_t)g.ntiles, &tkey2));
+  k_tile_keys<<<grid_for(g.ntiles, 256), 256, 0, st>>>(tile_cnt, g.ntiles, tkey, ord_in);
+  SDF_KERNEL(ctx);
+  {
+    size_t tmp_bytes = 0;
+    SDF_CUDA(ctx, cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_bytes, tkey, tkey2, ord_in, order, g.ntiles,
+                                                            0, 16, st));
+    void* tmp;
+    SDF_TRY(scratch(ctx, "cub_tmp_order", tmp_bytes, &tmp));
+    SDF_CUDA(ctx, cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_bytes, tkey, tkey2, ord_in, order, g.ntiles, 0,
+                                                            16, st));
+  }
 
   FoldArgs A;
   A.g = g;
   A.mode = mode;
   A.tile_off = tile_off;
   A.tile_cnt = tile_cnt;
+  A.order = order;
   A.vals = vals2;
   A.rec = rec;
   A.cent = cent;
