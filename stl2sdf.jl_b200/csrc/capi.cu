@@ -392,9 +392,16 @@ int sdfgpu_create(const sdfgpu_opts* opts, sdfgpu_ctx** out) {
   };
   if ((e = cudaSetDevice(dev)) != cudaSuccess) return bail("cudaSetDevice", e);
   if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail("cudaStreamCreate", e);
-  if ((e = cudaStreamCreateWithFlags(&ctx->sign_stream, cudaStreamNonBlocking)) != cudaSuccess)
+  // The sign stage and the LBVH build run beside the distance fold, whose launch queues thousands of
+  // CTAs: at the same priority their kernels would wait until the last fold CTA is dispatched.  At
+  // the highest priority the scheduler hands them SMs as fold CTAs retire, so they finish inside the
+  // fold instead of after it.
+  int prio_least = 0, prio_greatest = 0;
+  if ((e = cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest)) != cudaSuccess)
+    return bail("cudaDeviceGetStreamPriorityRange", e);
+  if ((e = cudaStreamCreateWithPriority(&ctx->sign_stream, cudaStreamNonBlocking, prio_greatest)) != cudaSuccess)
     return bail("cudaStreamCreate", e);
-  if ((e = cudaStreamCreateWithFlags(&ctx->bvh_stream, cudaStreamNonBlocking)) != cudaSuccess)
+  if ((e = cudaStreamCreateWithPriority(&ctx->bvh_stream, cudaStreamNonBlocking, prio_greatest)) != cudaSuccess)
     return bail("cudaStreamCreate", e);
   for (cudaEvent_t* ev : {&ctx->ev_fork, &ctx->ev_join, &ctx->ev_rows, &ctx->ev_mesh, &ctx->ev_bvh})
     if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return bail("cudaEventCreate", e);
