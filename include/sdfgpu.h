@@ -17,6 +17,8 @@
  *       src/MeshGrid/Grid.jl:9                             -> sdfgpu_grid_setup
  *   noninteractive_sdf_grid_setup(mesh, B)
  *       src/MeshGrid/Grid_setup.jl:104                     -> sdfgpu_grid_from_cell_size
+ *   analyze_mesh(calculate_edge_distances(mesh))
+ *       src/MeshGrid/Grid_setup.jl:28,64                   -> sdfgpu_mesh_edge_stats
  *   remove_sdf_artifacts!(sdf, grid; threshold, min_component_ratio)
  *       src/SignedDistances/SdfArtifactRemoval.jl:134      -> sdfgpu_remove_artifacts
  *   analyze_sdf_components(sdf, grid; threshold)
@@ -278,6 +280,16 @@ int sdfgpu_radius_eval(sdfgpu_ctx* ctx, const float* xn, int64_t B, float* dhat)
  * gradients against a CPU implementation. */
 int sdfgpu_mlp_train_eval(sdfgpu_ctx* ctx, const float* params, const float* xn, const float* target, int64_t B,
                           float* dhat, float* loss, float* grad);
+
+/* Edge-length statistics of the resident mesh, the analysis that calculate_edge_distances and
+ * analyze_mesh (src/MeshGrid/Grid_setup.jl:28-102) print before the grid step is chosen.  Edge i of
+ * a triangle runs from its vertex i to vertex i+1 (wrapping); lengths are FP64 norms of the vertex
+ * differences.  out[0] shortest edge, out[1] longest edge, out[2] mean edge length, out[3] median
+ * edge length (mean of the two middle values for an even count), out[4] / out[5] mean edge length
+ * of the triangle with the smallest / largest sum of edge lengths; idx_out (may be NULL) receives
+ * those two triangles' 0-based indices (the first one on ties, as Julia's argmin / argmax).
+ * Returns after the results are in out. */
+int sdfgpu_mesh_edge_stats(sdfgpu_ctx* ctx, double out[6], int64_t idx_out[2]);
 
 /* remove_sdf_artifacts!(sdf, grid; threshold, min_component_ratio)
  * (src/SignedDistances/SdfArtifactRemoval.jl:134-248), in place on the sdf of the grid with N cells

@@ -6,7 +6,9 @@
 * :class:`Grid` -- Grid.jl:9-32, computed by ``sdfgpu_grid_setup`` (the same host arithmetic the
   C ABI uses, so the Python object and the library always agree on the grid).
 * :func:`generateGridPoints` -- Grid.jl:82-96: node = AABB_min + cell_size * [i, j, k], x fastest.
-* :func:`noninteractive_sdf_grid_setup` / :func:`interactive_sdf_grid_setup` -- Grid_setup.jl.
+* :func:`noninteractive_sdf_grid_setup` / :func:`interactive_sdf_grid_setup` -- Grid_setup.jl,
+  including the mesh analysis they print first (:func:`mesh_edge_statistics`, computed on the GPU
+  by ``sdfgpu_mesh_edge_stats``).
 """
 
 from __future__ import annotations
@@ -132,8 +134,41 @@ def generateGridPoints(grid: Grid) -> GridPoints:
     return out
 
 
-def noninteractive_sdf_grid_setup(mesh: TriangularMesh, B: float) -> Grid:
-    """Grid_setup.jl:104-124: N_new = floor(max extent / B), 3 padding cells."""
+_RED, _BOLD, _RESET = "\x1b[31m", "\x1b[1m", "\x1b[0m"
+
+
+def mesh_edge_statistics(mesh: TriangularMesh, device: int = 0) -> dict:
+    """Edge-length statistics of the mesh (calculate_edge_distances + analyze_mesh,
+    Grid_setup.jl:28-102), computed on the GPU: shortest, longest, mean and median edge, and the mean
+    edge of the triangles with the smallest / largest edge sum (smallest_index / largest_index,
+    0-based, the first on ties).  Uploads the mesh to the device's default context, where the
+    distance and sign calls that follow find it."""
+    ctx = _native.default_context(device)
+    ctx.set_mesh(mesh.vertex_rows(), mesh.triangle_rows(), key=mesh._key)
+    return ctx.mesh_edge_stats()
+
+
+def analyze_mesh(mesh: TriangularMesh, device: int = 0) -> dict:
+    """Prints the mesh analysis of Grid_setup.jl:64-102 and returns its statistics."""
+    st = mesh_edge_statistics(mesh, device)
+    print("Mesh Statistics:")
+    print("----------------")
+    print(f"Number of elements: {mesh.nel}")
+    print(f"Shortest edge in the mesh: {_RED}{_BOLD}{round(st['shortest'], 4)}{_RESET}")
+    print(f"Longest edge in the mesh: {round(st['longest'], 4)}")
+    print(f"Average edge length: {round(st['mean'], 4)}")
+    print(f"Median edge length: {round(st['median'], 4)}")
+    print(f"Average edge length of the smallest element: {_RED}{_BOLD}{round(st['smallest_mean'], 4)}{_RESET}")
+    print(f"Average edge length of the largest element: {round(st['largest_mean'], 4)}")
+    return st
+
+
+def noninteractive_sdf_grid_setup(mesh: TriangularMesh, B: float, analyze: bool = True) -> Grid:
+    """Grid_setup.jl:104-124: N_new = floor(max extent / B), 3 padding cells.
+
+    analyze: print the mesh analysis first, as the reference does (needs the GPU)."""
+    if analyze:
+        analyze_mesh(mesh)
     o, amax, N, h, ngp = _native.grid_from_cell_size(mesh.vertex_rows(), float(B))
     g = Grid.from_parts(o, N, h)
     g.AABB_max = amax
@@ -141,13 +176,16 @@ def noninteractive_sdf_grid_setup(mesh: TriangularMesh, B: float) -> Grid:
     return g
 
 
-def interactive_sdf_grid_setup(mesh: TriangularMesh) -> Grid:
-    """Grid_setup.jl:126-173: prompts for the cell size on stdin until the user accepts."""
+def interactive_sdf_grid_setup(mesh: TriangularMesh, analyze: bool = True) -> Grid:
+    """Grid_setup.jl:126-173: prints the mesh analysis (analyze=True, needs the GPU), then prompts for
+    the cell size on stdin until the user accepts."""
+    if analyze:
+        analyze_mesh(mesh)
     while True:
         while True:
             try:
                 B = float(input("Write a grid step based on grid analysis: "))
-                g = noninteractive_sdf_grid_setup(mesh, B)
+                g = noninteractive_sdf_grid_setup(mesh, B, analyze=False)
                 break
             except ValueError:
                 print("Error: Please enter a valid floating-point number.")

@@ -121,6 +121,7 @@ SIGNATURES = {
                               ctypes.POINTER(ctypes.c_int32), _dp], ctypes.c_int),
     "sdfgpu_sdf_components": ([ctypes.c_void_p, _i64p, _dp, ctypes.c_double, ctypes.POINTER(ctypes.c_int32), _i64p,
                                _i64p], ctypes.c_int),
+    "sdfgpu_mesh_edge_stats": ([ctypes.c_void_p, _dp, _i64p], ctypes.c_int),
     "sdfgpu_get_stream": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "sdfgpu_get_stats": ([ctypes.c_void_p, ctypes.POINTER(Stats)], ctypes.c_int),
 }
@@ -397,6 +398,18 @@ class Context:
                                                 roots.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(c),
                                                 ctypes.byref(l)))
         return roots, c.value, l.value
+
+    # ---- mesh analysis (Grid_setup.jl:28-102) ----
+    def mesh_edge_stats(self):
+        """Edge-length statistics of the resident mesh: dict with shortest, longest, mean, median,
+        smallest_mean / largest_mean (mean edge of the triangle with the smallest / largest edge sum)
+        and smallest_index / largest_index (0-based)."""
+        out = np.empty(6, np.float64)
+        idx = np.empty(2, np.int64)
+        self._check(lib().sdfgpu_mesh_edge_stats(self._p, out.ctypes.data_as(_dp), idx.ctypes.data_as(_i64p)))
+        return {"shortest": float(out[0]), "longest": float(out[1]), "mean": float(out[2]), "median": float(out[3]),
+                "smallest_mean": float(out[4]), "largest_mean": float(out[5]), "smallest_index": int(idx[0]),
+                "largest_index": int(idx[1])}
 
     # ---- RBF smoothing (RBFs4Smoothing.jl) ----
     def rbf_smoothing(self, aabb_min, aabb_max, N, cell_size, dist, interpolation=True, smooth=2, threshold=1e-3,
