@@ -19,6 +19,8 @@
  *       src/MeshGrid/Grid_setup.jl:104                     -> sdfgpu_grid_from_cell_size
  *   analyze_mesh(calculate_edge_distances(mesh))
  *       src/MeshGrid/Grid_setup.jl:28,64                   -> sdfgpu_mesh_edge_stats
+ *   process_stl_mesh(vertices, triangles)
+ *       src/DataImport/ImportStlData.jl:198                -> sdfgpu_stl_dedupe
  *   remove_sdf_artifacts!(sdf, grid; threshold, min_component_ratio)
  *       src/SignedDistances/SdfArtifactRemoval.jl:134      -> sdfgpu_remove_artifacts
  *   analyze_sdf_components(sdf, grid; threshold)
@@ -290,6 +292,19 @@ int sdfgpu_mlp_train_eval(sdfgpu_ctx* ctx, const float* params, const float* xn,
  * those two triangles' 0-based indices (the first one on ties, as Julia's argmin / argmax).
  * Returns after the results are in out. */
 int sdfgpu_mesh_edge_stats(sdfgpu_ctx* ctx, double out[6], int64_t idx_out[2]);
+
+/* Vertex deduplication of the STL import, process_stl_mesh (src/DataImport/ImportStlData.jl:198-309).
+ * V holds the nv = 3 * nel vertices of the STL in stream order (x, y, z of each; triangle e is rows
+ * 3e, 3e+1, 3e+2).  Writes the unique vertices to X_out (room for nv rows of 3 doubles; *nnp_out
+ * rows used) in order of first appearance, and to IEN_out (nv entries) the 1-based index of every
+ * stream vertex, i.e. the 3 x nel triangle matrix.  Equal vertices merge (-0.0 equals +0.0).
+ * *near_out receives the number of ordered pairs of distinct unique vertices closer than 1e-10
+ * (norm): when it is zero the result is the reference's; otherwise the reference's order-dependent
+ * tolerance merge differs from exact deduplication and the caller must apply it.  Non-finite
+ * vertices, or coordinates whose hash cell floor(x * 1e10) is not an Int64, are errors (the
+ * reference throws for them too).  Returns after the results are in the host buffers. */
+int sdfgpu_stl_dedupe(sdfgpu_ctx* ctx, const double* V, int64_t nv, double* X_out, int64_t* IEN_out,
+                      int64_t* nnp_out, int64_t* near_out);
 
 /* remove_sdf_artifacts!(sdf, grid; threshold, min_component_ratio)
  * (src/SignedDistances/SdfArtifactRemoval.jl:134-248), in place on the sdf of the grid with N cells

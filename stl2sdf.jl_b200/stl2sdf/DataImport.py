@@ -13,8 +13,10 @@ array and the triangles as an ``(nel, 3)`` int64 array of 1-based indices (the r
   (dx outermost, then dy, then dz).  The unique vertices keep their first-appearance order.
   When no two distinct vertices lie within 1e-10 of each other (always the case for meshes
   whose coordinates are separated by more than that), the result equals exact deduplication in
-  first-appearance order, which is what the vectorised fast path computes; otherwise the
-  sequential restatement runs.
+  first-appearance order, which runs on the GPU (``sdfgpu_stl_dedupe``: radix sorts, a scan and
+  the reference's hash cells to detect distinct vertices closer than 1e-10).  Only when such
+  vertices exist does the reference's order-dependent merge apply; it is then walked on the host
+  (:func:`_dedupe_sequential`).
 """
 
 from __future__ import annotations
@@ -64,7 +66,9 @@ def read_ascii_stl(filename: str):
 
 
 def _dedupe_sequential(V: np.ndarray, T: np.ndarray):
-    """Literal restatement of process_stl_mesh (ImportStlData.jl:198-309)."""
+    """process_stl_mesh (ImportStlData.jl:198-309) walked vertex by vertex, for the meshes whose
+    distinct vertices come closer than 1e-10 (the GPU detects them), where the merge depends on the
+    stream order."""
     tol = 1e-10
     sf = 10000000000  # floor(Int, 1/tol)
     vmap: dict = {}
@@ -102,26 +106,19 @@ def _dedupe_sequential(V: np.ndarray, T: np.ndarray):
     return np.asarray(uniq, dtype=np.float64).reshape(-1, 3), newT
 
 
-def process_stl_mesh(V: np.ndarray, T: np.ndarray):
-    """Deduplicate vertices (ImportStlData.jl:198-309).  Returns (X, IEN), IEN 1-based."""
+def process_stl_mesh(V: np.ndarray, T: np.ndarray, device: int = 0):
+    """Deduplicate vertices (ImportStlData.jl:198-309) on the GPU.  Returns (X, IEN), IEN 1-based."""
+    from . import _native
+
     V = np.ascontiguousarray(V, dtype=np.float64).reshape(-1, 3)
     T = np.ascontiguousarray(T, dtype=np.int64).reshape(-1, 3)
     if not np.all(np.isfinite(V)):
         raise ValueError("STL vertices must be finite")
     if T.shape[0] == 0:
         return np.zeros((0, 3)), np.zeros((0, 3), dtype=np.int64)
-    stream = V[T.reshape(-1) - 1]
-    uniq, first, inv = np.unique(stream, axis=0, return_index=True, return_inverse=True)
-    order = np.argsort(first, kind="stable")
-    rank = np.empty_like(order)
-    rank[order] = np.arange(order.shape[0])
-    X = uniq[order]
-    IEN = (rank[inv.reshape(-1)] + 1).reshape(-1, 3).astype(np.int64)
-    if X.shape[0] > 1:
-        from scipy.spatial import cKDTree
-
-        if cKDTree(X).query_pairs(r=1e-10, output_type="ndarray").shape[0] > 0:
-            return _dedupe_sequential(V, T)
+    X, IEN, near = _native.default_context(device).stl_dedupe(V[T.reshape(-1) - 1])
+    if near:
+        return _dedupe_sequential(V, T)
     return X, IEN
 
 
@@ -152,9 +149,20 @@ def write_binary_stl(filename: str, X: np.ndarray, IEN: np.ndarray, header: byte
 
 
 def roundtrip_float32(X: np.ndarray, IEN: np.ndarray):
-    """(X, IEN) exactly as import_stl returns it after write_binary_stl, without touching disk."""
+    """(X, IEN) as import_stl returns it after write_binary_stl, without touching disk: the vertices
+    rounded to float32 and renumbered in order of first appearance in the triangle stream (unused
+    ones dropped).  For building workload meshes from generated ones, whose distinct vertices stay
+    distinct and farther apart than 1e-10 after the rounding (checked: an error otherwise)."""
     X = np.asarray(X, dtype=np.float64).reshape(-1, 3)
     F = np.asarray(IEN, dtype=np.int64).reshape(-1, 3) - 1
-    V = X[F.reshape(-1)].astype(np.float32).astype(np.float64)
-    T = np.arange(1, V.shape[0] + 1, dtype=np.int64).reshape(-1, 3)
-    return process_stl_mesh(V, T)
+    ids, first = np.unique(F.reshape(-1), return_index=True)
+    used = ids[np.argsort(first, kind="stable")]  # original ids in first-appearance order
+    new = np.empty(X.shape[0], np.int64)
+    new[used] = np.arange(1, used.shape[0] + 1)
+    X32 = X[used].astype(np.float32).astype(np.float64)
+    if X32.shape[0] > 1:
+        from scipy.spatial import cKDTree
+
+        if cKDTree(X32).query_pairs(r=1e-10, output_type="ndarray").shape[0] > 0:
+            raise ValueError("mesh vertices coincide (within 1e-10) after rounding to float32")
+    return X32, new[F]

@@ -122,6 +122,7 @@ SIGNATURES = {
     "sdfgpu_sdf_components": ([ctypes.c_void_p, _i64p, _dp, ctypes.c_double, ctypes.POINTER(ctypes.c_int32), _i64p,
                                _i64p], ctypes.c_int),
     "sdfgpu_mesh_edge_stats": ([ctypes.c_void_p, _dp, _i64p], ctypes.c_int),
+    "sdfgpu_stl_dedupe": ([ctypes.c_void_p, _dp, ctypes.c_int64, _dp, _i64p, _i64p, _i64p], ctypes.c_int),
     "sdfgpu_get_stream": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "sdfgpu_get_stats": ([ctypes.c_void_p, ctypes.POINTER(Stats)], ctypes.c_int),
 }
@@ -410,6 +411,18 @@ class Context:
         return {"shortest": float(out[0]), "longest": float(out[1]), "mean": float(out[2]), "median": float(out[3]),
                 "smallest_mean": float(out[4]), "largest_mean": float(out[5]), "smallest_index": int(idx[0]),
                 "largest_index": int(idx[1])}
+
+    # ---- STL import (ImportStlData.jl:198-309) ----
+    def stl_dedupe(self, stream):
+        """Deduplicate the (3 nel, 3) stream of STL vertices: (X (nnp, 3), IEN (nel, 3) 1-based, number
+        of ordered pairs of distinct vertices closer than 1e-10)."""
+        S = np.ascontiguousarray(stream, np.float64).reshape(-1, 3)
+        X = np.empty_like(S)
+        IEN = np.empty(S.shape[0], np.int64)
+        nnp, near = ctypes.c_int64(), ctypes.c_int64()
+        self._check(lib().sdfgpu_stl_dedupe(self._p, S.ctypes.data_as(_dp), S.shape[0], X.ctypes.data_as(_dp),
+                                            IEN.ctypes.data_as(_i64p), ctypes.byref(nnp), ctypes.byref(near)))
+        return X[:nnp.value].copy(), IEN.reshape(-1, 3), near.value
 
     # ---- RBF smoothing (RBFs4Smoothing.jl) ----
     def rbf_smoothing(self, aabb_min, aabb_max, N, cell_size, dist, interpolation=True, smooth=2, threshold=1e-3,

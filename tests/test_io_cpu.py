@@ -13,22 +13,27 @@ from conftest import GOLDEN
 
 
 def test_reference_fixture_import():
-    """The reference's own test input: 3,712 triangles, 1,890 unique vertices, closed."""
+    """The reference's own test input: 3,712 triangles, 1,890 unique vertices, closed (the reader
+    and the oracle's deduplication; the GPU deduplication is checked against it in the gpu tests)."""
+    from oracle import stl_dedupe
     from stl2sdf import DataImport, synthetic
 
-    X, IEN = DataImport.import_stl(os.path.join(GOLDEN, "artifacts.stl"))
+    V, T = DataImport.read_binary_stl(os.path.join(GOLDEN, "artifacts.stl"))
+    X, IEN = stl_dedupe.exact(V, T)
+    assert stl_dedupe.near_pairs(X) == 0
     assert IEN.shape == (3712, 3) and X.shape == (1890, 3)
     assert synthetic.is_closed(IEN)
     assert IEN.min() == 1 and IEN.max() == X.shape[0]
 
 
 def test_binary_roundtrip_and_first_appearance_order(tmp_path):
+    from oracle import stl_dedupe
     from stl2sdf import DataImport, synthetic
 
     V, F = synthetic.icosphere(2, jitter=0.01, seed=3)
     path = str(tmp_path / "s.stl")
     DataImport.write_binary_stl(path, V, F)
-    X, IEN = DataImport.import_stl(path)
+    X, IEN = stl_dedupe.exact(*DataImport.read_binary_stl(path))
     X2, IEN2 = DataImport.roundtrip_float32(V, F)
     assert np.array_equal(X, X2) and np.array_equal(IEN, IEN2)
     # vertices appear in the order the triangle stream first mentions them
@@ -46,19 +51,32 @@ def test_ascii_reader(tmp_path):
         f.write("solid t\n facet normal 0 0 1\n  outer loop\n   vertex 0 0 0\n   vertex 1 0 0\n   vertex 0 1 0\n"
                 "  endloop\n endfacet\n facet normal 0 0 1\n  outer loop\n   vertex 1 0 0\n   vertex 1 1 0\n"
                 "   vertex 0 1 0\n  endloop\n endfacet\nendsolid t\n")
-    X, IEN = DataImport.import_stl(path)
+    from oracle import stl_dedupe
+
+    assert DataImport.detect_stl_type(path)
+    X, IEN = stl_dedupe.exact(*DataImport.read_ascii_stl(path))
     assert X.shape == (4, 3) and IEN.tolist() == [[1, 2, 3], [2, 4, 3]]
 
 
-def test_dedupe_tolerance_path_matches_sequential():
+def test_dedupe_tolerance_restatements():
+    """The reference's walk merges a vertex 1e-11 from the origin into it; exact deduplication does
+    not, and the near-pair count tells the two cases apart.  The product's host walk for that case
+    agrees with the oracle's."""
+    from oracle import stl_dedupe
     from stl2sdf import DataImport
 
     V = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [1e-11, 0, 0], [1, 1, 0], [0, 1, 0]], dtype=np.float64)
     T = np.array([[1, 2, 3], [4, 5, 6]])
-    X, IEN = DataImport.process_stl_mesh(V, T)
-    Xs, IENs = DataImport._dedupe_sequential(V, T)
-    assert np.array_equal(X, Xs) and np.array_equal(IEN, IENs)
-    assert X.shape[0] == 4 and IEN[1, 0] == 1  # 1e-11 merged into the origin
+    Xs, IENs = stl_dedupe.sequential(V, T)
+    assert Xs.shape[0] == 4 and IENs.tolist() == [[1, 2, 3], [1, 4, 3]]  # 1e-11 merged into the origin
+    Xe, IENe = stl_dedupe.exact(V, T)
+    assert Xe.shape[0] == 5 and stl_dedupe.near_pairs(Xe) == 2
+    Xp, IENp = DataImport._dedupe_sequential(V, T)
+    assert np.array_equal(Xp, Xs) and np.array_equal(IENp, IENs)
+    # without near pairs the walk is exact deduplication
+    V2 = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [-0.0, 0, 0], [1, 1, 0], [0, 1, 0]], dtype=np.float64)
+    a, b = stl_dedupe.sequential(V2, T), stl_dedupe.exact(V2, T)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[1].tolist() == [[1, 2, 3], [1, 4, 3]]
 
 
 def test_vti_roundtrip(tmp_path):
