@@ -388,7 +388,7 @@ int sdfgpu_sdf_batch_ex(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count
     o.device = ctx->device;
     for (int a = 0; a < 3; ++a) o.tile[a] = ctx->tile[a];
     sdfgpu_ctx* w = nullptr;
-    if (sdfgpu_create(&o, &w) != SDFGPU_OK)
+    if (create_context(&o, &w, false) != SDFGPU_OK)
       return fail(ctx, SDFGPU_ERR_CUDA, std::string("batch worker: ") + sdfgpu_last_error(nullptr));
     ctx->workers.push_back(w);
   }

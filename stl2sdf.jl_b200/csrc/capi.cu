@@ -346,19 +346,10 @@ int sdf_host_impl(sdfgpu_ctx* ctx, const double origin[3], double h, const int64
   return SDFGPU_OK;
 }
 
-}  // namespace sdfgpu
-
-using namespace sdfgpu;
-
-extern "C" {
-
-int sdfgpu_abi_version(void) { return SDFGPU_ABI_VERSION; }
-
-const char* sdfgpu_last_error(const sdfgpu_ctx* ctx) {
-  return ctx ? ctx->err.c_str() : g_create_error.c_str();
-}
-
-int sdfgpu_create(const sdfgpu_opts* opts, sdfgpu_ctx** out) {
+// A context on device opts->device.  stage_priority: run the sign stage and the LBVH build on
+// high-priority streams (what sdfgpu_create does); the worker contexts of a batch share the GPU with
+// each other and use equal priorities (see batch.cu).
+int create_context(const sdfgpu_opts* opts, sdfgpu_ctx** out, bool stage_priority) {
   if (!out) return fail(nullptr, SDFGPU_ERR_INVALID_ARGUMENT, "out must not be NULL");
   *out = nullptr;
   int ndev = 0;
@@ -395,13 +386,16 @@ int sdfgpu_create(const sdfgpu_opts* opts, sdfgpu_ctx** out) {
   // The sign stage and the LBVH build run beside the distance fold, whose launch queues thousands of
   // CTAs: at the same priority their kernels would wait until the last fold CTA is dispatched.  At
   // the highest priority the scheduler hands them SMs as fold CTAs retire, so they finish inside the
-  // fold instead of after it.
+  // fold instead of after it.  Not for batch workers: with several contexts sharing the GPU, one
+  // worker's high-priority sign stage would hold back another's tile lists, which its host thread
+  // waits for, and the workers would overlap less.
   int prio_least = 0, prio_greatest = 0;
   if ((e = cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest)) != cudaSuccess)
     return bail("cudaDeviceGetStreamPriorityRange", e);
-  if ((e = cudaStreamCreateWithPriority(&ctx->sign_stream, cudaStreamNonBlocking, prio_greatest)) != cudaSuccess)
+  const int stage_prio = stage_priority ? prio_greatest : prio_least;
+  if ((e = cudaStreamCreateWithPriority(&ctx->sign_stream, cudaStreamNonBlocking, stage_prio)) != cudaSuccess)
     return bail("cudaStreamCreate", e);
-  if ((e = cudaStreamCreateWithPriority(&ctx->bvh_stream, cudaStreamNonBlocking, prio_greatest)) != cudaSuccess)
+  if ((e = cudaStreamCreateWithPriority(&ctx->bvh_stream, cudaStreamNonBlocking, stage_prio)) != cudaSuccess)
     return bail("cudaStreamCreate", e);
   for (cudaEvent_t* ev : {&ctx->ev_fork, &ctx->ev_join, &ctx->ev_rows, &ctx->ev_mesh, &ctx->ev_bvh})
     if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return bail("cudaEventCreate", e);
@@ -423,6 +417,20 @@ int sdfgpu_create(const sdfgpu_opts* opts, sdfgpu_ctx** out) {
   *out = ctx;
   return SDFGPU_OK;
 }
+
+}  // namespace sdfgpu
+
+using namespace sdfgpu;
+
+extern "C" {
+
+int sdfgpu_abi_version(void) { return SDFGPU_ABI_VERSION; }
+
+const char* sdfgpu_last_error(const sdfgpu_ctx* ctx) {
+  return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+int sdfgpu_create(const sdfgpu_opts* opts, sdfgpu_ctx** out) { return create_context(opts, out, true); }
 
 int sdfgpu_destroy(sdfgpu_ctx* ctx) {
   if (!ctx) return SDFGPU_OK;

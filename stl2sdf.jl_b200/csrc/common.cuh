@@ -197,6 +197,7 @@ __device__ __forceinline__ void count_add(int64_t* counters, int idx, int64_t v)
 
 // Call scaffolding of the entry points (capi.cu).
 int begin_call(sdfgpu_ctx* ctx);
+int create_context(const sdfgpu_opts* opts, sdfgpu_ctx** out, bool stage_priority);
 int need_mesh(sdfgpu_ctx* ctx);
 int reset_counters(sdfgpu_ctx* ctx);
 int finish_counters(sdfgpu_ctx* ctx, const GridP& g);
