@@ -44,13 +44,24 @@ class Options:
         self.distance_mode = distance_mode
 
 
-def stl_to_sdf(stl_filename: str, options: Options = None, out_dir: str = "."):
+def stl_to_sdf(stl_filename: str, options: Options = None, out_dir: str = ".", timings: dict = None):
     """stl_to_sdf (src/stl_to_sdf.jl:75-147): STL -> mesh -> grid -> distances x signs -> VTI.
 
     Writes ``<base>_sdf.vti`` (point field "distance") into out_dir, and with a smoothing method
     also ``<base>_fine_sdf.vti`` (the RBF-smoothed field on the refined grid, Float32).  Returns
-    (sdf, grid, path).
+    (sdf, grid, path).  timings: a dict to receive the host wall-clock seconds of each stage
+    ("import", "grid", "sdf", "artifacts", "export", "smoothing"; the stages that ran).
     """
+    import time
+
+    clock = [time.perf_counter()]
+
+    def lap(name):
+        now = time.perf_counter()
+        if timings is not None:
+            timings[name] = now - clock[0]
+        clock[0] = now
+
     options = options or Options()
     if options.smoothing_method is not None and options.smoothing_method not in ("interpolation", "approximation"):
         raise AssertionError("smoothing_method must be :interpolation, :approximation, or nothing")
@@ -61,20 +72,26 @@ def stl_to_sdf(stl_filename: str, options: Options = None, out_dir: str = "."):
     base = os.path.splitext(os.path.basename(stl_filename))[0]
     X, IEN = import_stl(stl_filename)
     mesh = TriangularMesh(X, IEN)
+    lap("import")
     if options.cell_size is None:
         grid = interactive_sdf_grid_setup(mesh)
     else:
         grid = noninteractive_sdf_grid_setup(mesh, float(options.cell_size))
+    lap("grid")
     sdf, dist, sign, conf = signed_distance_field(mesh, grid, mode=options.distance_mode)
+    lap("sdf")
     low = int(np.count_nonzero(conf < 0.6))
     if low:
         print(f"{low} points have low confidence (<0.6)")
     if options.remove_artifacts:
         flipped = remove_sdf_artifacts(sdf, grid, min_component_ratio=options.artifact_ratio)
         print(f"Artifact removal completed: {flipped} nodes modified")
+        lap("artifacts")
     path = exportSdfToVTI(os.path.join(out_dir, f"{base}_sdf.vti"), grid, sdf, "distance")
+    lap("export")
     if options.smoothing_method is not None:
         fine_sdf, fine_grid = RBFs_smoothing(sdf, grid, options.smoothing_method == "interpolation",
                                              options.grid_refinement)
         exportSdfToVTI(os.path.join(out_dir, f"{base}_fine_sdf.vti"), fine_grid, fine_sdf, "distance")
+        lap("smoothing")
     return sdf, grid, path

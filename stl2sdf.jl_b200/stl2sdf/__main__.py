@@ -2,7 +2,7 @@
 
     PYTHONPATH=stl2sdf.jl_b200 python -m stl2sdf part.stl --cell-size 0.5 [--remove-artifacts]
         [--artifact-ratio 0.01] [--smoothing interpolation|approximation] [--grid-refinement 1|2]
-        [--out-dir DIR]
+        [--out-dir DIR] [--timings]
 
 Writes <base>_sdf.vti (and <base>_fine_sdf.vti with smoothing) like the reference.
 """
@@ -24,11 +24,23 @@ def main(argv=None) -> int:
     ap.add_argument("--smoothing", choices=["interpolation", "approximation"], default=None)
     ap.add_argument("--grid-refinement", type=int, default=1)
     ap.add_argument("--out-dir", default=".")
+    ap.add_argument("--timings", action="store_true", help="print the wall-clock seconds of each stage")
     a = ap.parse_args(argv)
     opts = Options(smoothing_method=a.smoothing, grid_refinement=a.grid_refinement, cell_size=a.cell_size,
                    remove_artifacts=a.remove_artifacts, artifact_ratio=a.artifact_ratio)
-    sdf, grid, path = stl_to_sdf(a.stl, opts, out_dir=a.out_dir)
+    t = {}
+    if a.timings:  # the CUDA context first, so that its creation is not counted in the first stage
+        import time
+
+        from . import _native
+
+        t0 = time.perf_counter()
+        _native.default_context(0)
+        t["context"] = time.perf_counter() - t0
+    sdf, grid, path = stl_to_sdf(a.stl, opts, out_dir=a.out_dir, timings=t)
     print(f"{path}: {grid.ngp} nodes, sdf in [{sdf.min():.6g}, {sdf.max():.6g}]")
+    if a.timings:
+        print("stage seconds: " + ", ".join(f"{k} {v:.3f}" for k, v in t.items()))
     return 0
 
 
