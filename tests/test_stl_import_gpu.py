@@ -84,3 +84,14 @@ def test_errors(gpu_ctx):
         gpu_ctx.stl_dedupe(np.array([[0, 0, np.nan], [1, 0, 0], [0, 1, 0]], np.float64))
     with pytest.raises(_native.SdfGpuError, match="Int64"):  # floor(Int, 1e9 * 1e10) throws in the reference
         gpu_ctx.stl_dedupe(np.array([[1e9, 0, 0], [1, 0, 0], [0, 1, 0]], np.float64))
+
+
+def test_cli_reports_stage_timings(tmp_path, capsys):
+    from stl2sdf.__main__ import main
+
+    assert main([os.path.join(GOLDEN, "artifacts.stl"), "--cell-size", "0.5", "--timings",
+                 "--out-dir", str(tmp_path)]) == 0
+    out = capsys.readouterr().out
+    line = [x for x in out.splitlines() if x.startswith("stage seconds: ")]
+    assert line and all(k in line[0] for k in ("context", "import", "grid", "sdf", "export"))
+    assert os.path.exists(tmp_path / "artifacts_sdf.vti")
