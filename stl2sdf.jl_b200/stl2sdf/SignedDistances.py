@@ -68,11 +68,13 @@ def raycast_sign_detection(mesh: TriangularMesh, grid: Grid, points=None, min_ra
 
 
 def signed_distance_field(mesh: TriangularMesh, grid: Grid, mode: str = "ref", min_rays: int = 6, max_rays: int = 30,
-                          confidence_threshold: float = 0.6, use_winding_fallback: bool = True, device: int = 0):
-    """Fused ``dists .* signs`` (stl_to_sdf.jl:105-119) in one library call: (sdf, dist, sign, conf)."""
+                          confidence_threshold: float = 0.6, use_winding_fallback: bool = True, device: int = 0,
+                          parts=("dist", "sign", "conf")):
+    """Fused ``dists .* signs`` (stl_to_sdf.jl:105-119) in one library call: (sdf, dist, sign, conf).
+    Only the named parts are copied back to the host; the others are None."""
     ctx = _ctx(mesh, device)
     return ctx.sdf(grid.AABB_min, grid.cell_size, grid.N, MODES[mode], min_rays, max_rays, confidence_threshold,
-                   use_winding_fallback, want_parts=True)
+                   use_winding_fallback, want_parts=tuple(parts))
 
 
 def last_stats(device: int = 0) -> dict:

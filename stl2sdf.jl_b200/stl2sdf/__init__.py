@@ -78,7 +78,7 @@ def stl_to_sdf(stl_filename: str, options: Options = None, out_dir: str = ".", t
     else:
         grid = noninteractive_sdf_grid_setup(mesh, float(options.cell_size))
     lap("grid")
-    sdf, dist, sign, conf = signed_distance_field(mesh, grid, mode=options.distance_mode)
+    sdf, _, _, conf = signed_distance_field(mesh, grid, mode=options.distance_mode, parts=("conf",))
     lap("sdf")
     low = int(np.count_nonzero(conf < 0.6))
     if low:

@@ -245,11 +245,15 @@ class Context:
 
     def sdf(self, origin, h, N, mode=MODE_REF_RULE, min_rays=6, max_rays=30, confidence_threshold=0.6,
             use_winding_fallback=True, want_parts=False):
+        """sdf, or with want_parts (True, or a subset of ("dist", "sign", "conf")) the tuple
+        (sdf, dist, sign, conf) with None for the parts not asked for (they are not copied back)."""
         N = np.ascontiguousarray(N, np.int64)
         origin = np.ascontiguousarray(origin, np.float64)
         ngp = int(np.prod(N + 1))
         sdf = np.empty(ngp)
-        parts = [np.empty(ngp) for _ in range(3)] if want_parts else [None, None, None]
+        names = ("dist", "sign", "conf")
+        wanted = names if want_parts is True else (tuple(want_parts) if want_parts else ())
+        parts = [np.empty(ngp) if n in wanted else None for n in names]
         self._check(lib().sdfgpu_sdf(self._p, _d(origin), float(h), _i(N), int(mode), int(min_rays), int(max_rays),
                                      float(confidence_threshold), int(bool(use_winding_fallback)), _d(sdf),
                                      *[(_d(p) if p is not None else None) for p in parts]))
