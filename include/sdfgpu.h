@@ -75,7 +75,10 @@ typedef enum sdfgpu_distance_mode {
   /* True point-triangle minimum over all triangles, clamped to cell_size. */
   SDFGPU_MODE_EXACT = 1,
   /* True point-triangle minimum over all triangles, not clamped (a full unsigned distance). */
-  SDFGPU_MODE_UNBOUNDED = 2
+  SDFGPU_MODE_UNBOUNDED = 2,
+  /* SDFGPU_MODE_UNBOUNDED searched with the learned radius of the current mesh (train it first with
+   * sdfgpu_train_radius): the same bits as SDFGPU_MODE_UNBOUNDED.  No reference counterpart. */
+  SDFGPU_MODE_LEARNED = 3
 } sdfgpu_distance_mode;
 
 typedef struct sdfgpu_opts {
@@ -114,6 +117,8 @@ typedef struct sdfgpu_stats {
   int64_t certified_nodes;        /* learned radius: nodes whose bounded search certified the result */
   double radius_loss;             /* final training loss of the radius network */
   int64_t bvh_visits;             /* LBVH nodes visited by the unbounded search (one per warp and node) */
+  double ms_train;                /* device time of the last sdfgpu_train_radius (coarse grid + training) */
+  int64_t train_launches;         /* kernels of this library launched by the last sdfgpu_train_radius */
 } sdfgpu_stats;
 
 /* Context lifetime.  opts may be NULL (device 0, default tiles). */
@@ -190,11 +195,12 @@ int sdfgpu_sdf_slab_device(sdfgpu_ctx* ctx, const double origin[3], double h, co
  * GPU loading the library holds until the process exits, and calls no allocator.
  *   d_X (3 x nnp), d_IEN (3 x nel, 1-based) and d_dist_out (ngp doubles) are device memory of the
  *   current device; mode is SDFGPU_MODE_EXACT or SDFGPU_MODE_UNBOUNDED; stream may be NULL.
- *   At most 16384 triangles (SDFGPU_ERR_CAPACITY beyond).  The result equals sdfgpu_distances in
- *   the same mode.  Returns after the stream has finished; errors go to sdfgpu_last_error(NULL).
- *   Every call reuses the same array: calls that overlap on the GPU race, so serialise them.
- *   The first call on a device looks up the array's address with that device current; make it
- *   before any stream capture. */
+ *   At most 16384 triangles, and at most 2^36 (node, triangle) pairs: the work is one FP64 step
+ *   per pair (SDFGPU_ERR_CAPACITY beyond either).  The result equals sdfgpu_distances in the same
+ *   mode.  The call synchronizes `stream` before it returns, so it must not be made while that
+ *   stream is being captured.  Errors go to sdfgpu_last_error(NULL); when IEN holds an index
+ *   outside 1..nnp, d_dist_out is left as it was.  Every call reuses the same array: calls that
+ *   overlap on the GPU race, so serialise them. */
 int sdfgpu_distances_noalloc(const double* d_X, int64_t nnp, const int64_t* d_IEN, int64_t nel,
                              const double origin[3], double h, const int64_t N[3], int32_t mode,
                              double* d_dist_out, void* stream);
@@ -338,11 +344,6 @@ int sdfgpu_sdf_components(sdfgpu_ctx* ctx, const int64_t N[3], const double* sdf
 int sdfgpu_rbf_smoothing(sdfgpu_ctx* ctx, const double aabb_min[3], const double aabb_max[3], const int64_t N[3],
                          double cell_size, const double* dist, int32_t interpolation, int32_t smooth, double threshold,
                          float* fine_out, float* weights_out, int32_t* cg_iterations, double* cg_residual);
-
-/* Measured FP32 CUDA-core throughput of `device` in TFLOP/s (independent FMA chains on every SM at
- * full occupancy, best of five timed launches), the denominator of the hot path's FP32 roofline.
- * No counterpart in the reference. */
-int sdfgpu_measure_fp32_peak(int32_t device, double* tflops);
 
 /* The cudaStream_t every kernel of the context runs on. */
 int sdfgpu_get_stream(sdfgpu_ctx* ctx, void** stream);

@@ -350,6 +350,7 @@ int sdfgpu_autotune(sdfgpu_ctx* ctx, const double origin[3], double h, const int
   SDF_TRY(begin_call(ctx));
   SDF_TRY(need_mesh(ctx));
   SDF_TRY(check_mode(ctx, mode, 0));
+  if (mode == SDFGPU_MODE_LEARNED) mode = SDFGPU_MODE_UNBOUNDED;  // the learned search uses the same brick
   int32_t t[3];
   double ms = 0.0;
   SDF_TRY(autotune_tile(ctx, origin, h, N, mode, t, &ms));
@@ -373,6 +374,8 @@ int sdfgpu_sdf_batch_ex(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count
   if (count < 0 || (count > 0 && !items)) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "items must hold count entries");
   if (streams < 0 || streams > kMaxStreams)
     return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "streams must be in 0.." + std::to_string(kMaxStreams));
+  if (mode == SDFGPU_MODE_LEARNED)
+    return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "batches take modes 0..2 (SDFGPU_MODE_LEARNED needs a network per mesh)");
   SDF_TRY(check_mode(ctx, mode, 0));
   SDF_TRY(check_sign_args(ctx, min_rays, max_rays, confidence_threshold));
   for (int64_t i = 0; i < count; ++i) {

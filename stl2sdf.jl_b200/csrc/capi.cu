@@ -221,8 +221,10 @@ int check_sign_args(sdfgpu_ctx* ctx, int min_rays, int max_rays, double conf) {
 }
 
 int check_mode(sdfgpu_ctx* ctx, int mode, int learned) {
-  if (mode < SDFGPU_MODE_REF_RULE || mode > SDFGPU_MODE_UNBOUNDED)
+  if (mode < SDFGPU_MODE_REF_RULE || mode > SDFGPU_MODE_LEARNED)
     return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "unknown distance mode");
+  if (mode == SDFGPU_MODE_LEARNED && !ctx->radius.trained)
+    return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "SDFGPU_MODE_LEARNED: no radius network (sdfgpu_train_radius)");
   if (learned && mode != SDFGPU_MODE_UNBOUNDED)
     return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "use_learned_radius needs SDFGPU_MODE_UNBOUNDED");
   if (learned && !ctx->radius.trained)
@@ -234,6 +236,10 @@ int check_mode(sdfgpu_ctx* ctx, int mode, int learned) {
 int run_all(sdfgpu_ctx* ctx, const GridP& g, bool want_dist, bool want_sign, int mode, int learned, int min_rays,
             int max_rays, double conf, int use_winding, double* d_dist, double* d_xp, double* d_sign, double* d_conf,
             double* d_sdf, DistPlan* defer) {
+  if (mode == SDFGPU_MODE_LEARNED) {  // the unbounded search with the learned radius
+    mode = SDFGPU_MODE_UNBOUNDED;
+    learned = 1;
+  }
   SDF_TRY(reset_counters(ctx));
   ctx->launches = 0;
   for (int i = 0; i < T_NUM; ++i) SDF_MARK(ctx, i);
@@ -567,7 +573,17 @@ int sdfgpu_train_radius(sdfgpu_ctx* ctx, int32_t coarse_n, int32_t steps, int32_
   if (coarse_n < 9 || coarse_n > 1024 || steps < 0 || batch < 32 || !(lr > 0.f))
     return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "train_radius: need 9 <= coarse_n <= 1024, steps >= 0, batch >= 32, lr > 0");
   SDF_TRY(reset_counters(ctx));
-  return train_radius(ctx, coarse_n, steps, batch, lr, seed, final_loss);
+  ctx->launches = 0;
+  SDF_MARK(ctx, T_DIST0);
+  SDF_TRY(train_radius(ctx, coarse_n, steps, batch, lr, seed, final_loss));
+  SDF_MARK(ctx, T_DIST1);
+  SDF_CUDA(ctx, cudaEventSynchronize(ctx->tev[T_DIST1]));
+  float ms = 0.f;
+  SDF_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->tev[T_DIST0], ctx->tev[T_DIST1]));
+  ctx->stats.ms_train = ms;
+  ctx->stats.train_launches = ctx->launches;
+  ctx->stats.radius_loss = ctx->radius.loss;
+  return SDFGPU_OK;
 }
 
 int sdfgpu_radius_param_count(void) { return kParams; }

@@ -10,17 +10,20 @@
 //
 // Limits and sharing:
 //   * at most kNoAllocMaxTriangles triangles (larger meshes are rejected with an error);
+//   * the work is one FP64 step per (node, triangle) pair, so a call may hold the GPU for a long
+//     time: calls with more than kNoAllocMaxSteps pairs are rejected with an error;
 //   * the array lives in every GPU that loads the library, until the process exits;
 //   * every call reuses the same array and it keeps the last call's contents, so two calls that
 //     overlap on the GPU (different streams, or several host threads) race and corrupt each
 //     other -- callers must serialise them;
-//   * the first call on a device looks up the array's device address (cudaGetSymbolAddress) with
-//     that device current; make that first call before any stream capture begins.
+//   * every call looks up the array's address on the current device (cudaGetSymbolAddress, which
+//     allocates nothing), so nothing cached goes stale when a context is torn down and rebuilt;
+//   * the call synchronizes its stream before it returns (to read the error word), so it must not
+//     be called while that stream is being captured.
 //
 // Work: one thread per node folds every triangle in index order with the reference's FP64 step
 // (true minimum), so the result is bit-identical to sdfgpu_distances in the same mode.
 #include <cmath>
-#include <mutex>
 #include <string>
 
 #include "common.cuh"
@@ -30,14 +33,12 @@ namespace sdfgpu {
 namespace {
 
 constexpr int64_t kNoAllocMaxTriangles = 16384;
+constexpr double kNoAllocMaxSteps = 68719476736.0;  // 2^36 (node, triangle) FP64 steps, well under a second
 constexpr size_t kNoAllocBytes = 256 + sizeof(TriRec64) * (size_t)kNoAllocMaxTriangles;  // ~5.8 MB
 
 // The only scratch of sdfgpu_distances_noalloc: an error word in the first 256 bytes, then the
 // triangle records.  In host code this name is only a handle for cudaGetSymbolAddress.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
-
-std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[128] = {};
 
 __global__ void k_na_prep(const double* __restrict__ X, int64_t nnp, const int64_t* __restrict__ IEN, int64_t nel,
                           unsigned char* scratch) {
@@ -78,6 +79,7 @@ __global__ void k_na_prep(const double* __restrict__ X, int64_t nnp, const int64
 __global__ void __launch_bounds__(128) k_na_dist(const unsigned char* scratch, int64_t nel, GridP g, int clamp,
                                                  double* __restrict__ out) {
   const TriRec64* rec = reinterpret_cast<const TriRec64*>(scratch + 256);
+  if (*reinterpret_cast<const volatile int*>(scratch) != 0) return;  // bad index: leave the output as it was
   for (int64_t lin = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; lin < g.ngp; lin += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = lin % g.n[0], j = (lin / g.n[0]) % g.n[1], k = lin / (g.n[0] * g.n[1]);
     const d3 p = node_coord(g.o, g.h, i, j, k);
@@ -115,22 +117,15 @@ extern "C" int sdfgpu_distances_noalloc(const double* d_X, int64_t nnp, const in
     ngp_d *= (double)(N[a] + 1);
   }
   if (ngp_d > 2147483647.0) return fail(nullptr, SDFGPU_ERR_INVALID_ARGUMENT, "grid has more than 2^31-1 nodes");
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= 128)
-    return fail(nullptr, SDFGPU_ERR_NO_DEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (ngp_d * (double)nel > kNoAllocMaxSteps)
+    return fail(nullptr, SDFGPU_ERR_CAPACITY,
+                "sdfgpu_distances_noalloc: nodes x triangles exceeds 2^36 FP64 steps (use sdfgpu_distances)");
+  // The device address of the array on the current device, looked up on every call (host code
+  // may not use the symbol's name as an address).
   void* scratch = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {  // once per device, with that device current
-      e = cudaGetSymbolAddress(&g_noalloc_ptr[dev], g_noalloc_scratch);
-      if (e != cudaSuccess) {
-        g_noalloc_ptr[dev] = nullptr;
-        return fail(nullptr, SDFGPU_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-      }
-    }
-    scratch = g_noalloc_ptr[dev];
-  }
+  cudaError_t e = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
+  if (e != cudaSuccess)
+    return fail(nullptr, SDFGPU_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
   cudaStream_t st = (cudaStream_t)stream;
   GridP g{};
   for (int a = 0; a < 3; ++a) {
@@ -151,6 +146,7 @@ extern "C" int sdfgpu_distances_noalloc(const double* d_X, int64_t nnp, const in
   if ((e = cudaMemcpyAsync(&flag, scratch, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
       (e = cudaStreamSynchronize(st)) != cudaSuccess)
     return fail(nullptr, SDFGPU_ERR_CUDA, std::string("sdfgpu_distances_noalloc: ") + cudaGetErrorString(e));
-  if (flag) return fail(nullptr, SDFGPU_ERR_INVALID_ARGUMENT, "IEN holds an index outside 1..nnp");
+  if (flag)
+    return fail(nullptr, SDFGPU_ERR_INVALID_ARGUMENT, "IEN holds an index outside 1..nnp (d_dist_out left unchanged)");
   return SDFGPU_OK;
 }

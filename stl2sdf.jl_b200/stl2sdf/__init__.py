@@ -3,8 +3,7 @@
 Mirrors the reference module ``stl2sdf`` (src/stl2sdf.jl): ``stl_to_sdf(stl_filename;
 options=Options(...))`` plus the submodules ``DataImport``, ``MeshGrid``, ``SignedDistances`` and
 ``DataExport``.  The distance and sign stages run in libsdfgpu.so (hand-written CUDA for
-sm_100a); the Julia host code of the reference binds the same C ABI through ``ccall``
-(see INTEGRATION.md).
+sm_100a); the Julia host code of the reference binds the same C ABI through ``ccall``.
 """
 
 from __future__ import annotations

@@ -23,6 +23,7 @@ STATUS_NAMES = {
 MODE_REF_RULE = 0
 MODE_EXACT = 1
 MODE_UNBOUNDED = 2
+MODE_LEARNED = 3
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -49,7 +50,7 @@ class Stats(ctypes.Structure):
         ("launches", ctypes.c_int64), ("mesh_launches", ctypes.c_int64), ("ms_tiles", ctypes.c_double),
         ("ms_fold", ctypes.c_double), ("ms_rows", ctypes.c_double), ("ms_parity", ctypes.c_double),
         ("ms_vote", ctypes.c_double), ("certified_nodes", ctypes.c_int64), ("radius_loss", ctypes.c_double),
-        ("bvh_visits", ctypes.c_int64),
+        ("bvh_visits", ctypes.c_int64), ("ms_train", ctypes.c_double), ("train_launches", ctypes.c_int64),
     ]
 
     def as_dict(self):
@@ -111,7 +112,6 @@ SIGNATURES = {
                          ctypes.POINTER(ctypes.c_int32), _dp], ctypes.c_int),
     "sdfgpu_set_brick": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
     "sdfgpu_set_radius_margin": ([ctypes.c_void_p, ctypes.c_float, ctypes.c_float], ctypes.c_int),
-    "sdfgpu_measure_fp32_peak": ([ctypes.c_int32, _dp], ctypes.c_int),
     "sdfgpu_remove_artifacts": ([ctypes.c_void_p, _i64p, _dp, ctypes.c_double, ctypes.c_double, _i64p, _i64p, _i64p],
                                 ctypes.c_int),
     "sdfgpu_remove_artifacts_device": ([ctypes.c_void_p, _i64p, ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
@@ -452,15 +452,6 @@ class Context:
         s = Stats()
         self._check(lib().sdfgpu_get_stats(self._p, ctypes.byref(s)))
         return s.as_dict()
-
-
-def measure_fp32_peak(device: int = 0) -> float:
-    """Measured FP32 CUDA-core throughput of the device (TFLOP/s)."""
-    t = ctypes.c_double(0.0)
-    rc = lib().sdfgpu_measure_fp32_peak(int(device), ctypes.byref(t))
-    if rc:
-        raise SdfGpuError(rc, "sdfgpu_measure_fp32_peak failed")
-    return t.value
 
 
 _default_ctx = {}

@@ -74,10 +74,26 @@ def gather_zslabs(part: np.ndarray, N, group=None, device=None):
     return np.concatenate([outs[r][: sizes[r]].cpu().numpy() for r in range(world)])
 
 
+def local_device(device=None) -> int:
+    """CUDA ordinal of this rank's GPU: the index of `device` (a torch device, an int or a 'cuda:k'
+    string) when given, else LOCAL_RANK from the launcher's environment, else 0."""
+    import os
+
+    if device is None:
+        return int(os.environ.get("LOCAL_RANK", "0"))
+    if isinstance(device, int):
+        return device
+    if isinstance(device, str):
+        return int(device.split(":", 1)[1]) if ":" in device else 0
+    idx = getattr(device, "index", None)
+    return int(idx) if idx is not None else 0
+
+
 def sdf_zslab(X, IEN, origin, h, N, compute=None, group=None, device=None, **vote):
     """The whole sdf field of grid (origin, h, N) computed as z-slabs, one per rank, gathered on
     rank 0 (returned there; None elsewhere).  compute(k0, k1) -> slab values; the default builds a
-    context on this rank's GPU and calls sdfgpu_sdf_slab."""
+    context on this rank's GPU -- `device` when given, else the LOCAL_RANK torchrun sets (one process
+    per GPU), else GPU 0 -- and calls sdfgpu_sdf_slab."""
     import torch.distributed as dist
 
     world = dist.get_world_size(group)
@@ -86,7 +102,7 @@ def sdf_zslab(X, IEN, origin, h, N, compute=None, group=None, device=None, **vot
     if compute is None:
         from . import _native
 
-        ctx = _native.Context(0 if device is None else int(getattr(device, "index", 0) or 0))
+        ctx = _native.Context(local_device(device))
         ctx.set_mesh(X, IEN)
 
         def compute(k0, k1):

@@ -28,7 +28,8 @@ def pytest_configure(config):
 @pytest.fixture(scope="session")
 def icosphere_mesh():
     """Workload 1: icosphere L4 (5,120 triangles), radial jitter N(0, 0.01), seed 0, float32 STL."""
-    from stl2sdf import DataImport, synthetic
+    from stl2sdf import DataImport
+    from workloads import synthetic
 
     V, F = synthetic.icosphere(4, jitter=0.01, seed=0)
     return DataImport.roundtrip_float32(V, F)
@@ -37,7 +38,8 @@ def icosphere_mesh():
 @pytest.fixture(scope="session")
 def torus_mesh():
     """Workload 2: torus R=1, r=0.3, 512 x 128 quads (131,072 triangles), tube noise U(-2%,2%), seed 1."""
-    from stl2sdf import DataImport, synthetic
+    from stl2sdf import DataImport
+    from workloads import synthetic
 
     V, F = synthetic.torus(1.0, 0.3, 512, 128, 0.02, seed=1)
     return DataImport.roundtrip_float32(V, F)

@@ -17,7 +17,8 @@ pytestmark = pytest.mark.gpu
 
 
 def _batch(count, seed, k_lo, k_hi):
-    from stl2sdf import DataImport, _native, synthetic
+    from stl2sdf import DataImport, _native
+    from workloads import synthetic
 
     out = []
     for r in synthetic.uneven_batch(count, seed=seed, k_lo=k_lo, k_hi=k_hi):
@@ -100,7 +101,8 @@ def test_batch_reports_failing_item(gpu_ctx, small_batch):
 def _coarse_sphere_item():
     """80 large triangles on a fine grid: triangles reach farther than 1.5 cells from their
     centroids, so the 3-nearest-vertex fallback runs (inside the batch's graph)."""
-    from stl2sdf import DataImport, _native, synthetic
+    from stl2sdf import DataImport, _native
+    from workloads import synthetic
 
     X, IEN = DataImport.roundtrip_float32(*synthetic.icosphere(1, jitter=0.01, seed=4))
     o, _, N, h, _ = _native.grid_setup(X.min(0), X.max(0), 48 - 7, 3)
@@ -132,7 +134,8 @@ def test_workload_batch_items_match_oracle(gpu_ctx):
     the largest blob mesh and the coarsest blob mesh (big triangles on a fine grid: the
     nearest-vertex fallback) through the batch, in both forms, against the oracle on 1,500 seeded
     nodes each."""
-    from stl2sdf import DataImport, _native, synthetic
+    from stl2sdf import DataImport, _native
+    from workloads import synthetic
 
     recipes = synthetic.uneven_batch(256, seed=3)
     ico = [r for r in recipes if r["kind"] == "icosphere"]

@@ -109,7 +109,7 @@ def test_torus_sample(gpu_ctx, torus_mesh):
 
 
 def _open_box():
-    from stl2sdf import synthetic
+    from workloads import synthetic
 
     V, F = synthetic.box((0.0, 0.0, 0.0), (1.0, 0.7, 0.4))
     return V, F[2:]  # drop one face: rays through the hole disagree, winding fallback runs
@@ -230,7 +230,8 @@ def test_errors_are_reported(gpu_ctx):
 
 def test_blobs_small_full(gpu_ctx):
     """Marching-cubes blob mesh (16 blobs, 96^3 lattice) on a 64-node grid, every node."""
-    from stl2sdf import DataImport, synthetic
+    from stl2sdf import DataImport
+    from workloads import synthetic
 
     V, F = synthetic.blobs(16, seed=5, cells=96)
     X, IEN = DataImport.roundtrip_float32(V, F)
@@ -245,7 +246,8 @@ def test_blobs_small_full(gpu_ctx):
 def test_gyroid_small_full(gpu_ctx):
     """Capped gyroid sheet (one period, 48^3 lattice): thin walls, grazing axis rays, adaptive
     vote and winding fallback; every node of a 48-node grid."""
-    from stl2sdf import DataImport, synthetic
+    from stl2sdf import DataImport
+    from workloads import synthetic
 
     V, F = synthetic.gyroid(48, 0.04, 1.0)
     X, IEN = DataImport.roundtrip_float32(V, F)
@@ -264,7 +266,8 @@ def test_gyroid_small_full(gpu_ctx):
 def test_blobs_full_size_sample(gpu_ctx):
     """Workload 3 mesh (64 blobs at 512^3, ~1.4M triangles) on its 256-node grid: every node on the
     GPU, a seeded sample of 3,000 nodes in the oracle; plus size-independent properties."""
-    from stl2sdf import DataImport, synthetic
+    from stl2sdf import DataImport
+    from workloads import synthetic
 
     V, F = synthetic.blobs(64, seed=2, cells=512)
     X, IEN = DataImport.roundtrip_float32(V, F)
@@ -284,7 +287,8 @@ def test_gyroid_full_size_sample(gpu_ctx):
     """Workload 5 mesh (gyroid sheet at 384^3, ~5.7M triangles) on its 320-node grid: every node on
     the GPU; in the oracle 1,500 seeded uniform nodes plus 1,500 seeded nodes within one cell of the
     sheet (where grazing axis rays, edge/vertex hits and near-equidistant triangles are)."""
-    from stl2sdf import DataImport, synthetic
+    from stl2sdf import DataImport
+    from workloads import synthetic
 
     V, F = synthetic.gyroid(384, 0.04, 2.0)
     X, IEN = DataImport.roundtrip_float32(V, F)
@@ -343,8 +347,8 @@ def test_unbounded_brick_autotune(gpu_ctx, icosphere_mesh):
 
 
 def test_fp32_peak_probe():
-    from stl2sdf import _native
+    import workloads
 
-    t = _native.measure_fp32_peak(0)
+    t = workloads.measure_fp32_peak(0)
     # 148 SMs x 128 FP32 lanes x 2 FLOPs at 1.0-2.0 GHz: well inside (20, 100) TFLOP/s
     assert 20.0 < t < 100.0, t

@@ -16,7 +16,8 @@ def test_reference_fixture_import():
     """The reference's own test input: 3,712 triangles, 1,890 unique vertices, closed (the reader
     and the oracle's deduplication; the GPU deduplication is checked against it in the gpu tests)."""
     from oracle import stl_dedupe
-    from stl2sdf import DataImport, synthetic
+    from stl2sdf import DataImport
+    from workloads import synthetic
 
     V, T = DataImport.read_binary_stl(os.path.join(GOLDEN, "artifacts.stl"))
     X, IEN = stl_dedupe.exact(V, T)
@@ -28,7 +29,8 @@ def test_reference_fixture_import():
 
 def test_binary_roundtrip_and_first_appearance_order(tmp_path):
     from oracle import stl_dedupe
-    from stl2sdf import DataImport, synthetic
+    from stl2sdf import DataImport
+    from workloads import synthetic
 
     V, F = synthetic.icosphere(2, jitter=0.01, seed=3)
     path = str(tmp_path / "s.stl")
@@ -95,7 +97,7 @@ def test_vti_roundtrip(tmp_path):
 
 
 def test_workload_meshes():
-    from stl2sdf import synthetic
+    from workloads import synthetic
 
     V, F = synthetic.icosphere(4)
     assert V.shape == (2562, 3) and F.shape == (5120, 3) and synthetic.is_closed(F)
@@ -161,7 +163,8 @@ def test_artifact_labelling_matches_union_find():
 
 
 def test_malformed_stl_is_reported(tmp_path):
-    from stl2sdf import DataImport, synthetic
+    from stl2sdf import DataImport
+    from workloads import synthetic
 
     V, F = synthetic.icosphere(1)
     good = tmp_path / "good.stl"

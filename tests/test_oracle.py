@@ -113,7 +113,7 @@ def test_ray_directions():
 
 
 def test_winding_number_of_box():
-    from stl2sdf import synthetic
+    from workloads import synthetic
 
     X, IEN = synthetic.box((0, 0, 0), (1, 1, 1))
     s, w = oracle.winding(X, IEN, [[0.5, 0.5, 0.5], [2.0, 0.5, 0.5], [0.1, 0.9, 0.5]])
@@ -141,7 +141,8 @@ def test_sphere_signs_and_distances(icosphere_mesh):
 
 
 def test_unjittered_sphere_distance_bound():
-    from stl2sdf import DataImport, synthetic
+    from stl2sdf import DataImport
+    from workloads import synthetic
 
     V, F = synthetic.icosphere(3, jitter=0.0)
     X, IEN = DataImport.roundtrip_float32(V, F)

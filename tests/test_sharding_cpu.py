@@ -53,7 +53,8 @@ def _rank_main(rank, world, port, out_path):
     import torch.distributed as dist
 
     import oracle
-    from stl2sdf import DataImport, synthetic
+    from stl2sdf import DataImport
+    from workloads import synthetic
 
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -88,3 +89,18 @@ def test_zslab_gather_two_gloo_ranks(tmp_path):
     mp.start_processes(_rank_main, args=(2, _free_port(), out), nprocs=2, join=True, start_method="spawn")
     got, want = np.load(out)
     assert np.array_equal(got, want)
+
+
+def test_local_device_follows_the_launcher(monkeypatch):
+    """Without an explicit device every rank builds its context on its own GPU (LOCAL_RANK)."""
+    monkeypatch.setenv("LOCAL_RANK", "3")
+    assert sharding.local_device() == 3
+    monkeypatch.delenv("LOCAL_RANK")
+    assert sharding.local_device() == 0
+    assert sharding.local_device(5) == 5
+    assert sharding.local_device("cuda:2") == 2
+
+    class Dev:
+        index = 6
+
+    assert sharding.local_device(Dev()) == 6

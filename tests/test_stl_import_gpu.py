@@ -31,7 +31,8 @@ def test_reference_fixture(gpu_ctx):
 
 @pytest.mark.parametrize("which", ["icosphere", "torus"])
 def test_binary_file_matches_oracle_and_roundtrip(tmp_path, which):
-    from stl2sdf import DataImport, synthetic
+    from stl2sdf import DataImport
+    from workloads import synthetic
 
     V, F = synthetic.icosphere(4, jitter=0.01, seed=0) if which == "icosphere" else \
         synthetic.torus(1.0, 0.3, 512, 128, 0.02, seed=1)

@@ -1,14 +1,14 @@
-// peak.cu -- measured FP32 CUDA-core throughput of the device, the denominator of the hot path's
-// FP32 roofline (nodes/s bound = FP32 FLOP/s / algorithmic FLOPs per node).  No counterpart in the
-// reference.
+// fp32_peak.cu -- measured FP32 CUDA-core throughput of the device, the denominator of the hot
+// path's FP32 roofline (nodes/s bound = FP32 FLOP/s / algorithmic FLOPs per node).  A measurement
+// probe of the benchmark, built into workloads/_build/libfp32peak.so, not part of libsdfgpu.so.
 //
 // Every thread runs kChains independent FMA chains (enough to cover the FMA pipe's latency) for
 // `iters` iterations; the grid fills every SM at full occupancy.  FLOPs = 2 per FMA.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
 #include <algorithm>
 
-#include "common.cuh"
-
-namespace sdfgpu {
 namespace {
 
 constexpr int kChains = 8;
@@ -32,17 +32,15 @@ __global__ void __launch_bounds__(kThreads) k_fma_peak(float seed, int iters, fl
 }
 
 }  // namespace
-}  // namespace sdfgpu
 
-using namespace sdfgpu;
-
-extern "C" int sdfgpu_measure_fp32_peak(int32_t device, double* tflops) {
-  if (!tflops) return SDFGPU_ERR_INVALID_ARGUMENT;
+// 0 = ok, 1 = bad argument, 2 = no such device, 3 = a CUDA call failed.
+extern "C" int fp32_peak_tflops(int32_t device, double* tflops) {
+  if (!tflops) return 1;
   *tflops = 0.0;
   int prev = 0;
-  if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) return SDFGPU_ERR_NO_DEVICE;
+  if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) return 2;
   int sms = 0, per_sm = 0;
-  int rc = SDFGPU_OK;
+  int rc = 0;
   cudaStream_t st = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   float* sink = nullptr;
@@ -50,30 +48,30 @@ extern "C" int sdfgpu_measure_fp32_peak(int32_t device, double* tflops) {
   do {
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fma_peak, kThreads, 0) != cudaSuccess) {
-      rc = SDFGPU_ERR_CUDA;
+      rc = 3;
       break;
     }
     const int blocks = sms * std::max(per_sm, 1);
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess ||
         cudaMalloc(&sink, sizeof(float) * blocks) != cudaSuccess) {
-      rc = SDFGPU_ERR_CUDA;
+      rc = 3;
       break;
     }
     float best = 1e30f;
-    for (int rep = 0; rep < 6 && rc == SDFGPU_OK; ++rep) {  // first launch is a warm-up
+    for (int rep = 0; rep < 6 && rc == 0; ++rep) {  // first launch is a warm-up
       cudaEventRecord(e0, st);
       k_fma_peak<<<blocks, kThreads, 0, st>>>(1.0f, iters, sink);
       cudaEventRecord(e1, st);
       float ms = 0.f;
       if (cudaGetLastError() != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
           cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
-        rc = SDFGPU_ERR_CUDA;
+        rc = 3;
         break;
       }
       if (rep > 0) best = std::min(best, ms);
     }
-    if (rc == SDFGPU_OK) {
+    if (rc == 0) {
       const double flops = 2.0 * (double)blocks * kThreads * (double)iters * 16.0 * kChains;
       *tflops = flops / (best * 1e-3) / 1e12;
     }

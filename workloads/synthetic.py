@@ -125,7 +125,11 @@ def _meshgen():
         import ctypes
         import os
 
-        path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "lib", "libmeshgen.so")
+        path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_build", "libmeshgen.so")
+        if not os.path.exists(path):
+            import subprocess
+
+            subprocess.run(["make", "-s", "-C", os.path.dirname(os.path.abspath(__file__))], check=True)
         L = ctypes.CDLL(os.path.abspath(path))
         dp, i64p = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)
         L.mg_blobs.argtypes = [dp, dp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double]
