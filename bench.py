@@ -288,6 +288,12 @@ def run_batch(args, rank, world, local):
     # the same batch with the folds of all meshes in one persistent launch inside a CUDA graph
     ctx.sdf_batch(mine, out=outs, streams=args.streams, autotune=True, persistent=True)  # buffers
     pers, _ = timed(max(1, min(args.steps, 3)), streams=args.streams, autotune=True, persistent=True)
+    # the same batch in the learned-radius form: every mesh trains its own network inside the call
+    from stl2sdf import _native as _nat
+
+    ctx.sdf_batch(mine, out=outs, streams=args.streams, autotune=True, mode=_nat.MODE_LEARNED)  # tuning, buffers
+    lrn, _ = timed(1, streams=args.streams, autotune=True, mode=_nat.MODE_LEARNED)
+    lst = ctx.stats()
     total = sum(ngps)
     value = total * args.steps / dt
     line = {
@@ -307,6 +313,11 @@ def run_batch(args, rank, world, local):
         "persistent_graph_form": {"value": total * max(1, min(args.steps, 3)) / pers,
                                   "note": "sdfgpu_sdf_batch_ex(persistent=1): every fold in one persistent launch, "
                                           "captured with the epilogues in one CUDA graph"},
+        "learned_radius_form": {"value": total / lrn, "s": lrn, "train_ms_summed": lst["ms_train"],
+                                "certified_fraction": lst["certified_nodes"] / max(1, lst["ngp"]),
+                                "fallback_rate": lst["unbounded_fallbacks"] / max(1, lst["ngp"]),
+                                "note": "SDFGPU_MODE_LEARNED: unbounded distances, one radius network trained per "
+                                        "mesh inside the call (training time included)"},
         "first_call_s": t_tune,
         "stages_ms_summed": {k: st[k] for k in ("ms_mesh", "ms_tiles", "ms_fold", "ms_rows", "ms_parity", "ms_vote")},
         "counters_summed": {k: st[k] for k in ("tile_pairs", "fp64_evals", "row_hits", "undecided_nodes", "extra_rays",

@@ -119,6 +119,7 @@ typedef struct sdfgpu_stats {
   int64_t bvh_visits;             /* LBVH nodes visited by the unbounded search (one per warp and node) */
   double ms_train;                /* device time of the last sdfgpu_train_radius (coarse grid + training) */
   int64_t train_launches;         /* kernels of this library launched by the last sdfgpu_train_radius */
+  int64_t sign_band_reruns;       /* axis-row ray-triangle tests decided in FP64 (FP32 result inside its error band) */
 } sdfgpu_stats;
 
 /* Context lifetime.  opts may be NULL (device 0, default tiles). */
@@ -242,7 +243,11 @@ int sdfgpu_sdf_batch(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count, i
  * tile) work list, every item with its own tile) followed by each item's nearest-vertex fallback
  * and combine on the worker streams side by side; then the fields are copied out.  Items go to the
  * workers by a fixed longest-processing-time assignment, so repeated batches reuse their buffers.
- * Unbounded batches always run per item. */
+ * Unbounded and learned-radius batches always run per item.  With mode = SDFGPU_MODE_LEARNED
+ * every mesh gets its own radius network, trained right after its LBVH with the options of the last
+ * sdfgpu_train_radius on ctx (defaults: 400 steps, batch 4096, learning rate 3e-3, seed 0) on a
+ * coarse grid of min(64, K / 2) nodes on its longest axis (at least 16), K the nodes on the longest
+ * axis of the mesh's own grid; results equal SDFGPU_MODE_UNBOUNDED. */
 int sdfgpu_sdf_batch_ex(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count, int32_t mode, int32_t min_rays,
                         int32_t max_rays, double confidence_threshold, int32_t use_winding_fallback, int32_t streams,
                         int32_t autotune, int32_t persistent);

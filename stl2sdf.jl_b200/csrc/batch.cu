@@ -15,7 +15,10 @@
 //      item), followed by every item's 3-nearest-vertex fallback and combine -- the whole sequence
 //      captured in one CUDA graph and launched once;
 //   3. the fields are copied to the callers' buffers.
-// Unbounded batches keep the per-item pipeline (their search has no tile lists).
+// Unbounded batches keep the per-item pipeline (their search has no tile lists).  Learned-radius
+// batches (SDFGPU_MODE_LEARNED) too: every worker trains a network for each of its meshes (on a
+// coarse grid of at most half the mesh grid's nodes per axis) right after the mesh's LBVH, then
+// runs the learned search of that mesh.
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -80,7 +83,11 @@ void add_stats(sdfgpu_stats& a, const sdfgpu_stats& b) {
   a.ms_parity += b.ms_parity;
   a.ms_vote += b.ms_vote;
   a.certified_nodes += b.certified_nodes;
+  a.unbounded_fallbacks += b.unbounded_fallbacks;
   a.bvh_visits += b.bvh_visits;
+  a.ms_train += b.ms_train;
+  a.train_launches += b.train_launches;
+  a.sign_band_reruns += b.sign_band_reruns;
 }
 
 struct BatchJob {
@@ -89,6 +96,7 @@ struct BatchJob {
   std::vector<int64_t> order;
   int mode, min_rays, max_rays, use_winding, autotune;
   double conf;
+  RadiusNorm train;  // SDFGPU_MODE_LEARNED: the training options every mesh gets
   std::atomic<int64_t> next{0};
   std::atomic<bool> stop{false};
   std::mutex mu;  // guards rc, err, stats and parent->tuned
@@ -103,7 +111,8 @@ struct BatchJob {
 // in the unbounded mode (which has no tiles), with every warp brick of kBricks.
 int autotune_tile(sdfgpu_ctx* ctx, const double origin[3], double h, const int64_t N[3], int mode, int32_t best[3],
                   double* best_ms) {
-  const bool bricks = mode == SDFGPU_MODE_UNBOUNDED;
+  const bool bricks = mode == SDFGPU_MODE_UNBOUNDED || mode == SDFGPU_MODE_LEARNED;
+  const bool learned = mode == SDFGPU_MODE_LEARNED;  // the learned search itself (the network is trained)
   int32_t* shape = bricks ? ctx->brick : ctx->tile;
   const int32_t(*table)[3] = bricks ? kBricks : kTiles;
   const int count = bricks ? (int)(sizeof(kBricks) / sizeof(kBricks[0])) : (int)(sizeof(kTiles) / sizeof(kTiles[0]));
@@ -120,7 +129,8 @@ int autotune_tile(sdfgpu_ctx* ctx, const double origin[3], double h, const int64
     for (int rep = 0; rep < 2 && rc == 0; ++rep) {
       rc = reset_counters(ctx);
       if (rc == 0 && cudaEventRecord(ctx->ev[0], ctx->stream) != cudaSuccess) rc = SDFGPU_ERR_CUDA;
-      if (rc == 0) rc = run_distances(ctx, g, mode, 0, d_dist, nullptr);
+      if (rc == 0)
+        rc = run_distances(ctx, g, learned ? SDFGPU_MODE_UNBOUNDED : mode, learned ? 1 : 0, d_dist, nullptr);
       if (rc == 0 && cudaEventRecord(ctx->ev[1], ctx->stream) != cudaSuccess) rc = SDFGPU_ERR_CUDA;
       if (rc == 0) rc = finish_counters(ctx, g);
       float ms = 0.f;
@@ -151,7 +161,7 @@ int pick_tile(BatchJob& J, sdfgpu_ctx* w, const sdfgpu_batch_item& it) {
     std::lock_guard<std::mutex> lk(J.mu);
     auto f = J.parent->tuned.find(key);
     if (f != J.parent->tuned.end()) {
-      unpack_tile(f->second, J.mode == SDFGPU_MODE_UNBOUNDED ? w->brick : w->tile);
+      unpack_tile(f->second, (J.mode == SDFGPU_MODE_UNBOUNDED || J.mode == SDFGPU_MODE_LEARNED) ? w->brick : w->tile);
       return 0;
     }
   }
@@ -173,6 +183,14 @@ void worker_main(BatchJob& J, sdfgpu_ctx* w) {
     sdfgpu_batch_item& it = J.items[i];
     int rc = sdfgpu_set_mesh(w, it.X, it.nnp, it.IEN, it.nel);
     sdfgpu_stats ms = w->stats;
+    if (rc == 0 && J.mode == SDFGPU_MODE_LEARNED) {  // this mesh's network, on a coarse grid of its own
+      const int64_t K = std::max(it.N[0], std::max(it.N[1], it.N[2])) + 1;
+      const int coarse = (int)std::max<int64_t>(16, std::min<int64_t>(J.train.train_coarse, K / 2));
+      rc = sdfgpu_train_radius(w, coarse, J.train.train_steps, J.train.train_batch, J.train.train_lr,
+                               J.train.train_seed, nullptr);
+      ms.ms_train = w->stats.ms_train;
+      ms.train_launches = w->stats.train_launches;
+    }
     if (rc == 0 && J.autotune) rc = pick_tile(J, w, it);
     if (rc == 0)
       rc = sdfgpu_sdf(w, it.origin, it.h, it.N, J.mode, J.min_rays, J.max_rays, J.conf, J.use_winding, it.sdf, it.dist,
@@ -189,6 +207,8 @@ void worker_main(BatchJob& J, sdfgpu_ctx* w) {
     sdfgpu_stats s = w->stats;
     s.ms_mesh = ms.ms_mesh;
     s.mesh_launches = ms.mesh_launches;
+    s.ms_train = ms.ms_train;
+    s.train_launches = ms.train_launches;
     add_stats(J.stats, s);
   }
 }
@@ -235,6 +255,8 @@ void worker_prepare(BatchJob& J, sdfgpu_ctx* w, const std::vector<int64_t>& mine
     sdfgpu_stats s = w->stats;
     s.ms_mesh = ms.ms_mesh;
     s.mesh_launches = ms.mesh_launches;
+    s.ms_train = ms.ms_train;
+    s.train_launches = ms.train_launches;
     add_stats(J.stats, s);
   }
 }
@@ -350,7 +372,6 @@ int sdfgpu_autotune(sdfgpu_ctx* ctx, const double origin[3], double h, const int
   SDF_TRY(begin_call(ctx));
   SDF_TRY(need_mesh(ctx));
   SDF_TRY(check_mode(ctx, mode, 0));
-  if (mode == SDFGPU_MODE_LEARNED) mode = SDFGPU_MODE_UNBOUNDED;  // the learned search uses the same brick
   int32_t t[3];
   double ms = 0.0;
   SDF_TRY(autotune_tile(ctx, origin, h, N, mode, t, &ms));
@@ -374,9 +395,9 @@ int sdfgpu_sdf_batch_ex(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count
   if (count < 0 || (count > 0 && !items)) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "items must hold count entries");
   if (streams < 0 || streams > kMaxStreams)
     return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "streams must be in 0.." + std::to_string(kMaxStreams));
-  if (mode == SDFGPU_MODE_LEARNED)
-    return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "batches take modes 0..2 (SDFGPU_MODE_LEARNED needs a network per mesh)");
-  SDF_TRY(check_mode(ctx, mode, 0));
+  if (mode < SDFGPU_MODE_REF_RULE || mode > SDFGPU_MODE_LEARNED)
+    return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "unknown distance mode");
+  if (mode != SDFGPU_MODE_LEARNED) SDF_TRY(check_mode(ctx, mode, 0));  // a learned batch trains every mesh itself
   SDF_TRY(check_sign_args(ctx, min_rays, max_rays, confidence_threshold));
   for (int64_t i = 0; i < count; ++i) {
     const sdfgpu_batch_item& it = items[i];
@@ -404,6 +425,7 @@ int sdfgpu_sdf_batch_ex(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count
   J.conf = confidence_threshold;
   J.use_winding = use_winding_fallback;
   J.autotune = autotune;
+  J.train = ctx->radius;
   J.order.resize((size_t)count);
   std::iota(J.order.begin(), J.order.end(), (int64_t)0);
   std::stable_sort(J.order.begin(), J.order.end(),
@@ -416,7 +438,7 @@ int sdfgpu_sdf_batch_ex(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count
       }
   std::vector<std::thread> threads;
   threads.reserve(nw);
-  if (mode == SDFGPU_MODE_UNBOUNDED || !persistent) {  // per-item pipelines
+  if (mode == SDFGPU_MODE_UNBOUNDED || mode == SDFGPU_MODE_LEARNED || !persistent) {  // per-item pipelines
     for (int k = 0; k < nw; ++k) threads.emplace_back(worker_main, std::ref(J), ctx->workers[k]);
     for (auto& t : threads) t.join();
     ctx->stats = J.stats;

@@ -206,6 +206,7 @@ int finish_counters(sdfgpu_ctx* ctx, const GridP& g) {
   s.rho_max = ctx->mesh.rho_max;
   s.certified_nodes = c[C_CERTIFIED];
   s.bvh_visits = c[C_VISITS];
+  s.sign_band_reruns = c[C_SIGN_BAND];
   s.radius_loss = ctx->radius.loss;
   if (c[C_ERR_STACK]) return fail(ctx, SDFGPU_ERR_CAPACITY, "BVH traversal stack overflow");
   if (c[C_ERR_CAPACITY])
@@ -574,6 +575,12 @@ int sdfgpu_train_radius(sdfgpu_ctx* ctx, int32_t coarse_n, int32_t steps, int32_
     return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "train_radius: need 9 <= coarse_n <= 1024, steps >= 0, batch >= 32, lr > 0");
   SDF_TRY(reset_counters(ctx));
   ctx->launches = 0;
+  RadiusNorm& R = ctx->radius;
+  R.train_coarse = coarse_n;
+  R.train_steps = steps;
+  R.train_batch = batch;
+  R.train_lr = lr;
+  R.train_seed = seed;
   SDF_MARK(ctx, T_DIST0);
   SDF_TRY(train_radius(ctx, coarse_n, steps, batch, lr, seed, final_loss));
   SDF_MARK(ctx, T_DIST1);

@@ -47,6 +47,7 @@ enum Counter : int {
   C_LIST_WINDING,   // length of the winding list
   C_CERTIFIED,      // learned radius: nodes certified by the bounded search
   C_VISITS,         // LBVH nodes visited by the unbounded search
+  C_SIGN_BAND,      // ray-triangle decisions inside the FP32 band, replayed in FP64
   C_NUM = 32
 };
 
@@ -221,6 +222,8 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
                           bool device_ptrs);
 int ensure_ine(sdfgpu_ctx* ctx);
 int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, double* d_dist, double* d_xp);
+// The learned-radius nearest-triangle search (learned.cu) with one FP32 radius per node.
+int run_learned(sdfgpu_ctx* ctx, const GridP& g, const float* radius, double* d_dist, double* d_xp);
 
 // The reference-rule / h-bounded distance stage in parts (distance.cu), so a batch can run the folds
 // of many meshes in one launch: dist_prepare builds one mesh's tile lists and fold arguments,

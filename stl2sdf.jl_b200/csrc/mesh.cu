@@ -190,7 +190,9 @@ __global__ void k_karras(const unsigned long long* __restrict__ keys, int n, BNo
     else { left = gamma; int_parent[gamma] = i; }
     if (hi == gamma + 1) { right = kLeafBit | (gamma + 1); leaf_parent[gamma + 1] = i; }
     else { right = gamma + 1; int_parent[gamma + 1] = i; }
-    nodes[i].d = make_int4(left, right, 0, 0);
+    // d.z, d.w: the node's range of sorted leaves [lo, hi]; its left child covers [lo, gamma] and its
+    // right child [gamma + 1, hi], so a parent tells the size of both children's subtrees.
+    nodes[i].d = make_int4(left, right, lo, hi);
   }
 }
 
@@ -230,9 +232,27 @@ __global__ void k_single_root(const float4* __restrict__ box32, BNode* nodes, in
   nd.a = make_float4(lo.x, lo.y, lo.z, hi.x);
   nd.b = make_float4(hi.y, hi.z, 3.0e38f, 3.0e38f);
   nd.c = make_float4(3.0e38f, -3.0e38f, -3.0e38f, -3.0e38f);
-  nd.d = make_int4(kLeafBit | 0, kLeafBit | 0, -1, 0);
+  nd.d = make_int4(kLeafBit | 0, kLeafBit | 0, 0, 0);
   nodes[0] = nd;
   leaf_prim[0] = 0;
+}
+
+// Leaf-ordered copies for the learned-radius search, which reads runs of consecutive leaves: the
+// FP32 vertices (3 x float4, as v32) and the outward-rounded box (2 x float4, as box32) of the
+// triangle at each sorted leaf; the box's lo.w carries the triangle's index.
+__global__ void k_leaf_order(const int32_t* __restrict__ leaf_prim, const float4* __restrict__ v32,
+                             const float4* __restrict__ box32, int n, float4* __restrict__ lv32,
+                             float4* __restrict__ lbox) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int prim = leaf_prim[i];
+    lv32[3 * i] = v32[3 * prim];
+    lv32[3 * i + 1] = v32[3 * prim + 1];
+    lv32[3 * i + 2] = v32[3 * prim + 2];
+    float4 lo = box32[2 * prim];
+    lo.w = __int_as_float(prim);
+    lbox[2 * i] = lo;
+    lbox[2 * i + 1] = box32[2 * prim + 1];
+  }
 }
 
 __global__ void k_ine_count(const int64_t* __restrict__ IEN, int64_t nel, int32_t* __restrict__ cnt) {
@@ -365,6 +385,11 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
     k_refit<<<grid_for(n, 256), 256, 0, sb>>>(keys2, box32, n, nodes, int_parent, leaf_parent, flags, leaf_prim);
     SDF_KERNEL(ctx);
   }
+  float4 *lv32, *lbox;
+  SDF_TRY(scratch_t(ctx, "lv32", (size_t)n * 3, &lv32));
+  SDF_TRY(scratch_t(ctx, "lbox32", (size_t)n * 2, &lbox));
+  k_leaf_order<<<grid_for(n, 256), 256, 0, sb>>>(leaf_prim, v32, box32, n, lv32, lbox);
+  SDF_KERNEL(ctx);
   SDF_CUDA(ctx, cudaEventRecord(ctx->ev_bvh, sb));
   unsigned long long hrho = 0;
   SDF_CUDA(ctx, cudaMemcpyAsync(&hrho, bb + 7, sizeof(hrho), cudaMemcpyDeviceToHost, st));

@@ -55,139 +55,6 @@ __device__ __forceinline__ void features(float x0, float x1, float x2, float f[k
 __device__ __forceinline__ float softplus(float y) { return y > 20.f ? y : log1pf(expf(y)); }
 __device__ __forceinline__ float sigmoid(float y) { return 1.f / (1.f + expf(-y)); }
 
-// ---- training -----------------------------------------------------------------------------
-
-// Per-sample forward (the definition above) storing what the backward needs, plus the loss term
-// and dL/dy of every sample.
-__global__ void k_train_fwd(const float* __restrict__ P, const float* __restrict__ X, const float* __restrict__ T,
-                            int64_t B, float* __restrict__ H0, float* __restrict__ H1, float* __restrict__ H2,
-                            float* __restrict__ A3, float* __restrict__ GY, float* __restrict__ LOSS,
-                            float* __restrict__ YHAT) {
-  __shared__ float W[kParams];
-  for (int q = threadIdx.x; q < kParams; q += blockDim.x) W[q] = (q < kOffB1 || (q >= kOffW2 && q < kOffB2) ||
-                                                                   (q >= kOffW3 && q < kOffB3) || (q >= kOffW4 && q < kOffB4))
-                                                                      ? h16(P[q]) : P[q];
-  __syncthreads();
-  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < B; b += (int64_t)gridDim.x * blockDim.x) {
-    float f[kIn];
-    features(X[3 * b], X[3 * b + 1], X[3 * b + 2], f);
-    float h0[kIn], h1[kHid], h2[kHid], a3[kHid];
-    for (int j = 0; j < kIn; ++j) { h0[j] = h16(f[j]); H0[b * kIn + j] = h0[j]; }
-    for (int i = 0; i < kHid; ++i) {
-      float z = W[kOffB1 + i];
-      for (int j = 0; j < kIn; ++j) z = fmaf(W[kOffW1 + i * kIn + j], h0[j], z);
-      h1[i] = h16(fmaxf(z, 0.f));
-      H1[b * kHid + i] = h1[i];
-    }
-    for (int i = 0; i < kHid; ++i) {
-      float z = W[kOffB2 + i];
-      for (int j = 0; j < kHid; ++j) z = fmaf(W[kOffW2 + i * kHid + j], h1[j], z);
-      h2[i] = h16(fmaxf(z, 0.f));
-      H2[b * kHid + i] = h2[i];
-    }
-    for (int i = 0; i < kHid; ++i) {
-      float z = W[kOffB3 + i];
-      for (int j = 0; j < kHid; ++j) z = fmaf(W[kOffW3 + i * kHid + j], h2[j], z);
-      a3[i] = fmaxf(z, 0.f);
-      A3[b * kHid + i] = a3[i];
-    }
-    float y = W[kOffB4];
-    for (int j = 0; j < kHid; ++j) y = fmaf(W[kOffW4 + j], a3[j], y);
-    const float dh = softplus(y);
-    if (YHAT) YHAT[b] = dh;
-    if (T) {
-      const float r = logf(dh + kLogEps) - logf(T[b] + kLogEps);
-      LOSS[b] = r * r;
-      GY[b] = 2.f * r / (dh + kLogEps) * sigmoid(y) / (float)B;
-    }
-  }
-}
-
-// Per-sample backward through the layers: DZ3, DZ2, DZ1 (the relu masks use the stored
-// activations: a unit is active when its stored output is > 0).
-__global__ void k_train_bwd(const float* __restrict__ P, int64_t B, const float* __restrict__ H1,
-                            const float* __restrict__ H2, const float* __restrict__ A3, const float* __restrict__ GY,
-                            float* __restrict__ DZ1, float* __restrict__ DZ2, float* __restrict__ DZ3) {
-  __shared__ float W[kParams];
-  for (int q = threadIdx.x; q < kParams; q += blockDim.x) W[q] = q < kOffB4 ? h16(P[q]) : P[q];
-  __syncthreads();
-  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < B; b += (int64_t)gridDim.x * blockDim.x) {
-    const float gy = GY[b];
-    float dz3[kHid], dz2[kHid];
-    for (int i = 0; i < kHid; ++i) {
-      dz3[i] = A3[b * kHid + i] > 0.f ? gy * W[kOffW4 + i] : 0.f;
-      DZ3[b * kHid + i] = dz3[i];
-    }
-    for (int j = 0; j < kHid; ++j) {
-      float s = 0.f;
-      for (int i = 0; i < kHid; ++i) s = fmaf(W[kOffW3 + i * kHid + j], dz3[i], s);
-      dz2[j] = H2[b * kHid + j] > 0.f ? s : 0.f;
-      DZ2[b * kHid + j] = dz2[j];
-    }
-    for (int j = 0; j < kHid; ++j) {
-      float s = 0.f;
-      for (int i = 0; i < kHid; ++i) s = fmaf(W[kOffW2 + i * kHid + j], dz2[i], s);
-      DZ1[b * kHid + j] = H1[b * kHid + j] > 0.f ? s : 0.f;
-    }
-  }
-}
-
-// Weight gradients: one CTA per output row of a layer; thread j sums DZ[b][row] * H[b][j] over
-// the batch in order (deterministic); thread 0 also sums the bias gradient.
-__global__ void k_train_wgrad(int64_t B, const float* __restrict__ H0, const float* __restrict__ H1,
-                              const float* __restrict__ H2, const float* __restrict__ A3, const float* __restrict__ GY,
-                              const float* __restrict__ DZ1, const float* __restrict__ DZ2,
-                              const float* __restrict__ DZ3, float* __restrict__ G) {
-  const int row = blockIdx.x;  // 0..63 layer 1, 64..127 layer 2, 128..191 layer 3, 192 layer 4
-  const int layer = row / kHid;
-  const int i = row % kHid;
-  const float* H;
-  const float* DZ;
-  int K, offW, offB;
-  if (layer == 0) { H = H0; DZ = DZ1; K = kIn; offW = kOffW1; offB = kOffB1; }
-  else if (layer == 1) { H = H1; DZ = DZ2; K = kHid; offW = kOffW2; offB = kOffB2; }
-  else if (layer == 2) { H = H2; DZ = DZ3; K = kHid; offW = kOffW3; offB = kOffB3; }
-  else { H = A3; DZ = GY; K = kHid; offW = kOffW4; offB = kOffB4; }
-  const int dzs = layer == 3 ? 1 : kHid;
-  const int dzo = layer == 3 ? 0 : i;
-  const int j = threadIdx.x;
-  if (j < K) {
-    float s = 0.f;
-    for (int64_t b = 0; b < B; ++b) s = fmaf(DZ[b * dzs + dzo], H[b * K + j], s);
-    G[offW + (layer == 3 ? j : i * K + j)] = s;
-  }
-  if (j == kHid) {
-    float s = 0.f;
-    for (int64_t b = 0; b < B; ++b) s += DZ[b * dzs + dzo];
-    G[offB + (layer == 3 ? 0 : i)] = s;
-  }
-}
-
-__global__ void k_adam(float* __restrict__ P, const float* __restrict__ G, float* __restrict__ M1,
-                       float* __restrict__ M2, int n, float lr, float b1t, float b2t) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n) return;
-  const float g = G[q];
-  const float m = 0.9f * M1[q] + 0.1f * g;
-  const float v = 0.999f * M2[q] + 0.001f * g * g;
-  M1[q] = m;
-  M2[q] = v;
-  P[q] -= lr * (m / (1.f - b1t)) / (sqrtf(v / (1.f - b2t)) + 1e-8f);
-}
-
-__global__ void k_reduce_loss(const float* __restrict__ L, int64_t B, float* out) {
-  __shared__ float red[256];
-  float s = 0.f;
-  for (int64_t b = threadIdx.x; b < B; b += blockDim.x) s += L[b];
-  red[threadIdx.x] = s;
-  __syncthreads();
-  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
-    if ((int)threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) *out = red[0] / (float)B;
-}
-
 // Training samples: nodes of the coarse grid (normalised) and their exact distances (normalised).
 __global__ void k_make_samples(const double* __restrict__ dist, GridP g, double cx, double cy, double cz, double s,
                                float* __restrict__ X, float* __restrict__ T) {
@@ -198,16 +65,6 @@ __global__ void k_make_samples(const double* __restrict__ dist, GridP g, double 
     X[3 * lin + 1] = (float)((p.y - cy) / s);
     X[3 * lin + 2] = (float)((p.z - cz) / s);
     T[lin] = (float)(dist[lin] / s);
-  }
-}
-
-__global__ void k_gather_batch(const float* __restrict__ X, const float* __restrict__ T,
-                               const int32_t* __restrict__ perm, int64_t off, int64_t B, float* __restrict__ XB,
-                               float* __restrict__ TB) {
-  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < B; b += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t q = perm[off + b];
-    XB[3 * b] = X[3 * q]; XB[3 * b + 1] = X[3 * q + 1]; XB[3 * b + 2] = X[3 * q + 2];
-    TB[b] = T[q];
   }
 }
 
@@ -256,6 +113,319 @@ __device__ __forceinline__ void acc_to_a(const float acc[8][4], uint32_t a[4][4]
     a[kc][2] = pack_h2(fmaxf(acc[2 * kc + 1][0], 0.f), fmaxf(acc[2 * kc + 1][1], 0.f));
     a[kc][3] = pack_h2(fmaxf(acc[2 * kc + 1][2], 0.f), fmaxf(acc[2 * kc + 1][3], 0.f));
   }
+}
+
+// ---- training (mma.sync m16n8k16, FP16 operands, FP32 accumulate) ------------------------------
+//
+// One step = k_train_step + k_train_reduce.  k_train_step: every CTA takes kTS samples of the
+// step's batch (4 warps x 32).  A warp runs the forward of its 32 samples as three 64-wide GEMM
+// layers on the tensor cores (the inference kernel's fragments), the loss and dL/dy, then the
+// backward input gradients dZ3 -> dZ2 -> dZ1 as two more GEMMs (dH = dZ W, W read transposed from
+// shared memory), staging every activation and every dZ in shared memory as FP16.  Then each warp
+// forms a 16-row slice of every weight gradient dW = dZ^T H as GEMMs over the CTA's kTS samples,
+// and the CTA writes its partial gradient (and partial loss) to global memory.  k_train_reduce sums
+// the partials of all CTAs in a fixed order (deterministic), rescales, and applies Adam.
+//
+// dL/dy is carried scaled by kGyScale instead of 1/B so the FP16 dZ stay in range; the reduce
+// multiplies by 1 / (kGyScale B).  dZ beyond the FP16 range are clamped (only possible far from a
+// trained state; the gradient then stays finite).
+constexpr int kTS = 128;                 // samples per CTA
+constexpr float kGyScale = 1.f / 256.f;  // per-sample dL/dy scale inside the step
+constexpr int kLd1 = kIn + 8;            // shared-memory row strides in halves (padding against bank conflicts)
+constexpr int kLdH = kHid + 8;
+constexpr int kPart = kParams + 1;       // partial gradient of one CTA + its loss sum
+
+struct TrainSmem {
+  __half W1[kHid * kLd1];  // row major [out][in], FP16-rounded weights
+  __half W2[kHid * kLdH];
+  __half W3[kHid * kLdH];
+  float b1[kHid], b2[kHid], b3[kHid], w4[kHid];
+  float b4;
+  __half H0[kTS * kLd1];   // per sample: features, h1, h2 (the forward's FP16 activations)
+  __half H1[kTS * kLdH];
+  __half H2[kTS * kLdH];
+  __half D1[kTS * kLdH];   // per sample: dZ1, dZ2, dZ3 (scaled by kGyScale)
+  __half D2[kTS * kLdH];
+  __half D3[kTS * kLdH];
+  float gw4[4][kHid];
+  float red[4][2];         // per warp: sum of dL/dy (b4) and of the loss terms
+};
+
+__device__ __forceinline__ uint32_t pack_hh(__half lo, __half hi) {
+  __half2 v = __halves2half2(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+__device__ __forceinline__ float hclamp(float x) { return fminf(fmaxf(x, -60000.f), 60000.f); }
+
+// Accumulators of two adjacent n8 tiles -> the A fragment of one k16 tile (no activation).
+__device__ __forceinline__ void acc_to_a_raw(const float acc[8][4], uint32_t a[4][4]) {
+#pragma unroll
+  for (int kc = 0; kc < 4; ++kc) {
+    a[kc][0] = pack_h2(hclamp(acc[2 * kc][0]), hclamp(acc[2 * kc][1]));
+    a[kc][1] = pack_h2(hclamp(acc[2 * kc][2]), hclamp(acc[2 * kc][3]));
+    a[kc][2] = pack_h2(hclamp(acc[2 * kc + 1][0]), hclamp(acc[2 * kc + 1][1]));
+    a[kc][3] = pack_h2(hclamp(acc[2 * kc + 1][2]), hclamp(acc[2 * kc + 1][3]));
+  }
+}
+
+// Store an accumulator fragment (rows r0 and r0 + 8 of the tile) as FP16 into a row-major array.
+__device__ __forceinline__ void store_acc(__half* M, int ld, int r0, const uint32_t a[4][4], int t) {
+#pragma unroll
+  for (int kc = 0; kc < 4; ++kc) {
+    *reinterpret_cast<uint32_t*>(M + r0 * ld + 16 * kc + 2 * t) = a[kc][0];
+    *reinterpret_cast<uint32_t*>(M + (r0 + 8) * ld + 16 * kc + 2 * t) = a[kc][1];
+    *reinterpret_cast<uint32_t*>(M + r0 * ld + 16 * kc + 8 + 2 * t) = a[kc][2];
+    *reinterpret_cast<uint32_t*>(M + (r0 + 8) * ld + 16 * kc + 8 + 2 * t) = a[kc][3];
+  }
+}
+
+// acc = dZ (16 x 64, A fragments) x W (64 x 64 row major [out][in]): dH[s][in] = sum_out dZ[s][out] W[out][in].
+__device__ __forceinline__ void mma_back(const uint32_t a[4][4], const __half* W, float acc[8][4], int g, int t) {
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt) {
+    acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+#pragma unroll
+    for (int kc = 0; kc < 4; ++kc) {
+      const int k0 = 16 * kc + 2 * t, n = 8 * nt + g;
+      const uint32_t bf[2] = {pack_hh(W[k0 * kLdH + n], W[(k0 + 1) * kLdH + n]),
+                              pack_hh(W[(k0 + 8) * kLdH + n], W[(k0 + 9) * kLdH + n])};
+      mma16816(acc[nt], a[kc], bf);
+    }
+  }
+}
+
+// dZ masked by the activation of the forward (unit active when its stored FP16 output is > 0).
+__device__ __forceinline__ void mask_by(float acc[8][4], const __half* H, int r0, int t) {
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt) {
+    const int c = 8 * nt + 2 * t;
+    if (!(__half2float(H[r0 * kLdH + c]) > 0.f)) acc[nt][0] = 0.f;
+    if (!(__half2float(H[r0 * kLdH + c + 1]) > 0.f)) acc[nt][1] = 0.f;
+    if (!(__half2float(H[(r0 + 8) * kLdH + c]) > 0.f)) acc[nt][2] = 0.f;
+    if (!(__half2float(H[(r0 + 8) * kLdH + c + 1]) > 0.f)) acc[nt][3] = 0.f;
+  }
+}
+
+// dW rows [16 w, 16 w + 16) of one layer: sum over the CTA's kTS samples of dZ[s][out] H[s][in]
+// (A = dZ^T, B = H), written to the CTA's partial at offW (row stride K).
+template <int NT>
+__device__ __forceinline__ void wgrad_rows(const __half* D, const __half* H, int ldh, int K, int w, int g, int t,
+                                           float* out) {
+  float acc[NT][4];
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+  const int o = 16 * w + g;
+#pragma unroll 2
+  for (int kk = 0; kk < kTS / 16; ++kk) {
+    const int s0 = 16 * kk + 2 * t;
+    const uint32_t a[4] = {pack_hh(D[s0 * kLdH + o], D[(s0 + 1) * kLdH + o]),
+                           pack_hh(D[s0 * kLdH + o + 8], D[(s0 + 1) * kLdH + o + 8]),
+                           pack_hh(D[(s0 + 8) * kLdH + o], D[(s0 + 9) * kLdH + o]),
+                           pack_hh(D[(s0 + 8) * kLdH + o + 8], D[(s0 + 9) * kLdH + o + 8])};
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      const int n = 8 * nt + g;
+      const uint32_t bf[2] = {pack_hh(H[s0 * ldh + n], H[(s0 + 1) * ldh + n]),
+                              pack_hh(H[(s0 + 8) * ldh + n], H[(s0 + 9) * ldh + n])};
+      mma16816(acc[nt], a, bf);
+    }
+  }
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) {
+    const int c = 8 * nt + 2 * t;
+    out[o * K + c] = acc[nt][0];
+    out[o * K + c + 1] = acc[nt][1];
+    out[(o + 8) * K + c] = acc[nt][2];
+    out[(o + 8) * K + c + 1] = acc[nt][3];
+  }
+}
+
+// Forward, loss and backward of kTS samples per CTA; writes the CTA's partial gradient.  Sample q of
+// the step is X[perm[off + q]] (perm may be NULL: X[q]); samples q >= B contribute nothing.
+// dhat_out / loss_out (nullable) receive the per-sample network output and loss term.
+__global__ void __launch_bounds__(128) k_train_step(const float* __restrict__ P, const float* __restrict__ X,
+                                                    const float* __restrict__ T, const int32_t* __restrict__ perm,
+                                                    int64_t off, int64_t B, float* __restrict__ partial,
+                                                    float* __restrict__ dhat_out, float* __restrict__ loss_out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TrainSmem& S = *reinterpret_cast<TrainSmem*>(smem_raw);
+  for (int q = threadIdx.x; q < kHid * kIn; q += blockDim.x)
+    S.W1[(q / kIn) * kLd1 + q % kIn] = __float2half_rn(P[kOffW1 + q]);
+  for (int q = threadIdx.x; q < kHid * kHid; q += blockDim.x) {
+    S.W2[(q / kHid) * kLdH + q % kHid] = __float2half_rn(P[kOffW2 + q]);
+    S.W3[(q / kHid) * kLdH + q % kHid] = __float2half_rn(P[kOffW3 + q]);
+  }
+  for (int q = threadIdx.x; q < kHid; q += blockDim.x) {
+    S.b1[q] = P[kOffB1 + q];
+    S.b2[q] = P[kOffB2 + q];
+    S.b3[q] = P[kOffB3 + q];
+    S.w4[q] = h16(P[kOffW4 + q]);
+  }
+  if (threadIdx.x == 0) S.b4 = P[kOffB4];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int64_t cbase = (int64_t)blockIdx.x * kTS;
+  {  // features of this warp's 32 samples
+    const int sl = 32 * warp + lane;
+    const int64_t q = cbase + sl;
+    float x0 = 0.f, x1 = 0.f, x2 = 0.f;
+    if (q < B) {
+      const int64_t src = perm ? (int64_t)perm[off + q] : q;
+      x0 = X[3 * src]; x1 = X[3 * src + 1]; x2 = X[3 * src + 2];
+    }
+    float f[kIn];
+    features(x0, x1, x2, f);
+#pragma unroll
+    for (int j = 0; j < kIn; ++j) S.H0[sl * kLd1 + j] = __float2half_rn(f[j]);
+  }
+  __syncthreads();
+  float gw4[8][2];
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt) gw4[nt][0] = gw4[nt][1] = 0.f;
+  float gb4 = 0.f, lsum = 0.f;
+#pragma unroll 1
+  for (int mt = 0; mt < 2; ++mt) {
+    const int r0 = 32 * warp + 16 * mt + g;  // this thread's rows r0 and r0 + 8 (CTA-local samples)
+    uint32_t a1[2][4];
+#pragma unroll
+    for (int kc = 0; kc < 2; ++kc) {
+      const __half* p0 = &S.H0[r0 * kLd1 + 16 * kc + 2 * t];
+      const __half* p1 = &S.H0[(r0 + 8) * kLd1 + 16 * kc + 2 * t];
+      a1[kc][0] = *reinterpret_cast<const uint32_t*>(p0);
+      a1[kc][1] = *reinterpret_cast<const uint32_t*>(p1);
+      a1[kc][2] = *reinterpret_cast<const uint32_t*>(p0 + 8);
+      a1[kc][3] = *reinterpret_cast<const uint32_t*>(p1 + 8);
+    }
+    float acc[8][4];
+    uint32_t a2[4][4];
+    mma_layer<2>(a1, S.W1, kLd1, S.b1, acc, g, t);
+    acc_to_a(acc, a2);
+    store_acc(S.H1, kLdH, r0, a2, t);
+    mma_layer<4>(a2, S.W2, kLdH, S.b2, acc, g, t);
+    acc_to_a(acc, a2);
+    store_acc(S.H2, kLdH, r0, a2, t);
+    mma_layer<4>(a2, S.W3, kLdH, S.b3, acc, g, t);
+    // a3 = relu(acc); y = w4 . a3 + b4 for rows r0 (y0) and r0 + 8 (y1)
+    float y0 = 0.f, y1 = 0.f;
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[nt][e] = fmaxf(acc[nt][e], 0.f);
+      const float w0 = S.w4[8 * nt + 2 * t], w1 = S.w4[8 * nt + 2 * t + 1];
+      y0 = fmaf(w0, acc[nt][0], fmaf(w1, acc[nt][1], y0));
+      y1 = fmaf(w0, acc[nt][2], fmaf(w1, acc[nt][3], y1));
+    }
+    y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
+    y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
+    y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
+    y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
+    float gy[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const float y = (h == 0 ? y0 : y1) + S.b4;
+      const int64_t q = cbase + r0 + 8 * h;
+      float gq = 0.f;
+      if (q < B) {
+        const float dh = softplus(y);
+        if (dhat_out && t == 0) dhat_out[q] = dh;
+        if (T) {  // without targets (outputs only) nothing flows back
+          const float tq = T[perm ? (int64_t)perm[off + q] : q];
+          const float r = logf(dh + kLogEps) - logf(tq + kLogEps);
+          gq = 2.f * r / (dh + kLogEps) * sigmoid(y) * kGyScale;
+          if (t == 0) {
+            lsum += r * r;
+            gb4 += gq;
+            if (loss_out) loss_out[q] = r * r;
+          }
+        }
+      }
+      gy[h] = gq;
+    }
+    // dZ3 = [a3 > 0] gy w4, and the w4 gradient gy a3
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      const float w0 = S.w4[8 * nt + 2 * t], w1 = S.w4[8 * nt + 2 * t + 1];
+      gw4[nt][0] = fmaf(gy[0], acc[nt][0], fmaf(gy[1], acc[nt][2], gw4[nt][0]));
+      gw4[nt][1] = fmaf(gy[0], acc[nt][1], fmaf(gy[1], acc[nt][3], gw4[nt][1]));
+      acc[nt][0] = acc[nt][0] > 0.f ? gy[0] * w0 : 0.f;
+      acc[nt][1] = acc[nt][1] > 0.f ? gy[0] * w1 : 0.f;
+      acc[nt][2] = acc[nt][2] > 0.f ? gy[1] * w0 : 0.f;
+      acc[nt][3] = acc[nt][3] > 0.f ? gy[1] * w1 : 0.f;
+    }
+    uint32_t ad[4][4];
+    acc_to_a_raw(acc, ad);
+    store_acc(S.D3, kLdH, r0, ad, t);
+    __syncwarp();
+    mma_back(ad, S.W3, acc, g, t);  // dH2
+    mask_by(acc, S.H2, r0, t);      // dZ2
+    acc_to_a_raw(acc, ad);
+    store_acc(S.D2, kLdH, r0, ad, t);
+    mma_back(ad, S.W2, acc, g, t);  // dH1
+    mask_by(acc, S.H1, r0, t);      // dZ1
+    acc_to_a_raw(acc, ad);
+    store_acc(S.D1, kLdH, r0, ad, t);
+  }
+  // w4 gradient: sum over the 8 row groups g of the warp, then over the warps
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      float v = gw4[nt][e];
+      v += __shfl_xor_sync(0xffffffffu, v, 4);
+      v += __shfl_xor_sync(0xffffffffu, v, 8);
+      v += __shfl_xor_sync(0xffffffffu, v, 16);
+      if (g == 0) S.gw4[warp][8 * nt + 2 * t + e] = v;
+    }
+  for (int off2 = 16; off2 > 0; off2 >>= 1) {
+    gb4 += __shfl_xor_sync(0xffffffffu, gb4, off2);
+    lsum += __shfl_xor_sync(0xffffffffu, lsum, off2);
+  }
+  if (lane == 0) {
+    S.red[warp][0] = gb4;
+    S.red[warp][1] = lsum;
+  }
+  __syncthreads();
+  float* out = partial + (int64_t)blockIdx.x * kPart;
+  wgrad_rows<8>(S.D3, S.H2, kLdH, kHid, warp, g, t, out + kOffW3);
+  wgrad_rows<8>(S.D2, S.H1, kLdH, kHid, warp, g, t, out + kOffW2);
+  wgrad_rows<4>(S.D1, S.H0, kLd1, kIn, warp, g, t, out + kOffW1);
+  for (int q = threadIdx.x; q < 3 * kHid; q += blockDim.x) {  // bias gradients: sums of dZ over the samples
+    const int layer = q / kHid, o = q % kHid;
+    const __half* D = layer == 0 ? S.D1 : (layer == 1 ? S.D2 : S.D3);
+    float s = 0.f;
+    for (int sl = 0; sl < kTS; ++sl) s += __half2float(D[sl * kLdH + o]);
+    out[(layer == 0 ? kOffB1 : (layer == 1 ? kOffB2 : kOffB3)) + o] = s;
+  }
+  if (threadIdx.x < kHid)
+    out[kOffW4 + threadIdx.x] =
+        S.gw4[0][threadIdx.x] + S.gw4[1][threadIdx.x] + S.gw4[2][threadIdx.x] + S.gw4[3][threadIdx.x];
+  if (threadIdx.x == 0) {
+    out[kOffB4] = S.red[0][0] + S.red[1][0] + S.red[2][0] + S.red[3][0];
+    out[kParams] = S.red[0][1] + S.red[1][1] + S.red[2][1] + S.red[3][1];
+  }
+}
+
+// Sums the CTAs' partials in CTA order, scales them to dL/dP, and (adam = 1) applies one Adam step
+// at learning rate lr with the bias corrections b1t = 0.9^t, b2t = 0.999^t; G (nullable) receives
+// the gradient and *loss (nullable) the mean loss of the step.
+__global__ void k_train_reduce(const float* __restrict__ partial, int nparts, int64_t B, float* __restrict__ P,
+                               float* __restrict__ M1, float* __restrict__ M2, int adam, float lr, float b1t,
+                               float b2t, float* __restrict__ G, float* __restrict__ loss) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q > kParams) return;
+  float s = 0.f;
+  for (int c = 0; c < nparts; ++c) s += partial[(int64_t)c * kPart + q];
+  if (q == kParams) {
+    if (loss) *loss = s / (float)B;
+    return;
+  }
+  const float gq = s / (kGyScale * (float)B);
+  if (G) G[q] = gq;
+  if (!adam) return;
+  const float m = 0.9f * M1[q] + 0.1f * gq;
+  const float v = 0.999f * M2[q] + 0.001f * gq * gq;
+  M1[q] = m;
+  M2[q] = v;
+  P[q] -= lr * (m / (1.f - b1t)) / (sqrtf(v / (1.f - b2t)) + 1e-8f);
 }
 
 struct RadiusArgs {
@@ -350,6 +520,12 @@ __global__ void __launch_bounds__(128) k_radius(RadiusArgs A) {
 
 }  // namespace
 
+// k_train_step's shared memory (~128 KB) is above the default 48 KB limit.
+int train_smem_attr(sdfgpu_ctx* ctx) {
+  SDF_CUDA(ctx, cudaFuncSetAttribute(k_train_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainSmem)));
+  return 0;
+}
+
 int radius_params_init(sdfgpu_ctx* ctx, uint64_t seed) {
   // He-style uniform initialisation from a 64-bit LCG (deterministic per seed).
   std::vector<float> P(kParams, 0.f);
@@ -375,43 +551,30 @@ int radius_params_init(sdfgpu_ctx* ctx, uint64_t seed) {
   return 0;
 }
 
-// Forward (+ backward) of the training definition over B host samples; for gradient checks.
+// The training step's forward (+ backward) over B host samples at host params, without the update;
+// for checking the GPU gradients against a CPU implementation.
 int mlp_eval_host(sdfgpu_ctx* ctx, const float* params, const float* xn, const float* target, int64_t B, float* yhat,
                   float* loss, float* grad) {
   cudaStream_t st = ctx->stream;
-  float *dP, *dX, *dT, *H0, *H1, *H2, *A3, *GY, *LS, *YH, *DZ1, *DZ2, *DZ3, *G, *dl;
+  float *dP, *dX, *dT = nullptr, *YH, *G, *dl, *part;
+  const int nparts = (int)cdiv(B, kTS);
   SDF_TRY(scratch_t(ctx, "mlpe_p", kParams, &dP));
   SDF_TRY(scratch_t(ctx, "mlpe_x", (size_t)B * 3, &dX));
-  SDF_TRY(scratch_t(ctx, "mlpe_t", (size_t)B, &dT));
-  SDF_TRY(scratch_t(ctx, "mlpe_h0", (size_t)B * kIn, &H0));
-  SDF_TRY(scratch_t(ctx, "mlpe_h1", (size_t)B * kHid, &H1));
-  SDF_TRY(scratch_t(ctx, "mlpe_h2", (size_t)B * kHid, &H2));
-  SDF_TRY(scratch_t(ctx, "mlpe_a3", (size_t)B * kHid, &A3));
-  SDF_TRY(scratch_t(ctx, "mlpe_gy", (size_t)B, &GY));
-  SDF_TRY(scratch_t(ctx, "mlpe_ls", (size_t)B, &LS));
+  if (target) SDF_TRY(scratch_t(ctx, "mlpe_t", (size_t)B, &dT));
   SDF_TRY(scratch_t(ctx, "mlpe_yh", (size_t)B, &YH));
-  SDF_TRY(scratch_t(ctx, "mlpe_dz1", (size_t)B * kHid, &DZ1));
-  SDF_TRY(scratch_t(ctx, "mlpe_dz2", (size_t)B * kHid, &DZ2));
-  SDF_TRY(scratch_t(ctx, "mlpe_dz3", (size_t)B * kHid, &DZ3));
   SDF_TRY(scratch_t(ctx, "mlpe_g", kParams, &G));
   SDF_TRY(scratch_t(ctx, "mlpe_l", 1, &dl));
+  SDF_TRY(scratch_t(ctx, "mlpe_part", (size_t)nparts * kPart, &part));
   SDF_CUDA(ctx, cudaMemcpyAsync(dP, params, sizeof(float) * kParams, cudaMemcpyHostToDevice, st));
   SDF_CUDA(ctx, cudaMemcpyAsync(dX, xn, sizeof(float) * 3 * B, cudaMemcpyHostToDevice, st));
   if (target) SDF_CUDA(ctx, cudaMemcpyAsync(dT, target, sizeof(float) * B, cudaMemcpyHostToDevice, st));
-  k_train_fwd<<<grid_for(B, 128), 128, 0, st>>>(dP, dX, target ? dT : nullptr, B, H0, H1, H2, A3, GY, LS, YH);
+  SDF_TRY(train_smem_attr(ctx));
+  k_train_step<<<nparts, 128, sizeof(TrainSmem), st>>>(dP, dX, dT, nullptr, 0, B, part, YH, nullptr);
   SDF_KERNEL(ctx);
-  if (target) {
-    k_reduce_loss<<<1, 256, 0, st>>>(LS, B, dl);
-    SDF_KERNEL(ctx);
-    if (grad) {
-      k_train_bwd<<<grid_for(B, 128), 128, 0, st>>>(dP, B, H1, H2, A3, GY, DZ1, DZ2, DZ3);
-      SDF_KERNEL(ctx);
-      k_train_wgrad<<<3 * kHid + 1, 96, 0, st>>>(B, H0, H1, H2, A3, GY, DZ1, DZ2, DZ3, G);
-      SDF_KERNEL(ctx);
-      SDF_CUDA(ctx, cudaMemcpyAsync(grad, G, sizeof(float) * kParams, cudaMemcpyDeviceToHost, st));
-    }
-    if (loss) SDF_CUDA(ctx, cudaMemcpyAsync(loss, dl, sizeof(float), cudaMemcpyDeviceToHost, st));
-  }
+  k_train_reduce<<<(kPart + 255) / 256, 256, 0, st>>>(part, nparts, B, dP, nullptr, nullptr, 0, 0.f, 0.f, 0.f, G, dl);
+  SDF_KERNEL(ctx);
+  if (target && grad) SDF_CUDA(ctx, cudaMemcpyAsync(grad, G, sizeof(float) * kParams, cudaMemcpyDeviceToHost, st));
+  if (target && loss) SDF_CUDA(ctx, cudaMemcpyAsync(loss, dl, sizeof(float), cudaMemcpyDeviceToHost, st));
   if (yhat) SDF_CUDA(ctx, cudaMemcpyAsync(yhat, YH, sizeof(float) * B, cudaMemcpyDeviceToHost, st));
   SDF_CUDA(ctx, cudaStreamSynchronize(st));
   return 0;
@@ -466,48 +629,33 @@ int train_radius(sdfgpu_ctx* ctx, int coarse_n, int steps, int batch, float lr, 
   SDF_TRY(scratch_t(ctx, "mlp_perm", (size_t)ngp, &dperm));
   SDF_CUDA(ctx, cudaMemcpyAsync(dperm, perm.data(), sizeof(int32_t) * ngp, cudaMemcpyHostToDevice, st));
   SDF_TRY(radius_params_init(ctx, seed));
-  float *P, *M1, *M2, *XB, *TB, *H0, *H1, *H2, *A3, *GY, *LS, *DZ1, *DZ2, *DZ3, *G, *dl;
+  float *P, *M1, *M2, *part, *dl;
+  const int nparts = (int)cdiv(B, kTS);
   P = buf<float>(ctx, "mlp_p");
   SDF_TRY(scratch_t(ctx, "mlp_m1", kParams, &M1));
   SDF_TRY(scratch_t(ctx, "mlp_m2", kParams, &M2));
-  SDF_TRY(scratch_t(ctx, "mlp_xb", (size_t)B * 3, &XB));
-  SDF_TRY(scratch_t(ctx, "mlp_tb", (size_t)B, &TB));
-  SDF_TRY(scratch_t(ctx, "mlp_h0", (size_t)B * kIn, &H0));
-  SDF_TRY(scratch_t(ctx, "mlp_h1", (size_t)B * kHid, &H1));
-  SDF_TRY(scratch_t(ctx, "mlp_h2", (size_t)B * kHid, &H2));
-  SDF_TRY(scratch_t(ctx, "mlp_a3", (size_t)B * kHid, &A3));
-  SDF_TRY(scratch_t(ctx, "mlp_gy", (size_t)B, &GY));
-  SDF_TRY(scratch_t(ctx, "mlp_ls", (size_t)B, &LS));
-  SDF_TRY(scratch_t(ctx, "mlp_dz1", (size_t)B * kHid, &DZ1));
-  SDF_TRY(scratch_t(ctx, "mlp_dz2", (size_t)B * kHid, &DZ2));
-  SDF_TRY(scratch_t(ctx, "mlp_dz3", (size_t)B * kHid, &DZ3));
-  SDF_TRY(scratch_t(ctx, "mlp_g", kParams, &G));
+  SDF_TRY(scratch_t(ctx, "mlp_part", (size_t)nparts * kPart, &part));
   SDF_TRY(scratch_t(ctx, "mlp_l", 1, &dl));
   SDF_CUDA(ctx, cudaMemsetAsync(M1, 0, sizeof(float) * kParams, st));
   SDF_CUDA(ctx, cudaMemsetAsync(M2, 0, sizeof(float) * kParams, st));
+  SDF_TRY(train_smem_attr(ctx));
   float b1t = 1.f, b2t = 1.f;
   for (int it = 0; it < steps; ++it) {
     const int64_t off = (it % per_epoch) * B;
-    k_gather_batch<<<grid_for(B, 256), 256, 0, st>>>(X, T, dperm, off, B, XB, TB);
-    SDF_KERNEL(ctx);
-    k_train_fwd<<<grid_for(B, 128), 128, 0, st>>>(P, XB, TB, B, H0, H1, H2, A3, GY, LS, nullptr);
-    SDF_KERNEL(ctx);
-    k_train_bwd<<<grid_for(B, 128), 128, 0, st>>>(P, B, H1, H2, A3, GY, DZ1, DZ2, DZ3);
-    SDF_KERNEL(ctx);
-    k_train_wgrad<<<3 * kHid + 1, 96, 0, st>>>(B, H0, H1, H2, A3, GY, DZ1, DZ2, DZ3, G);
+    k_train_step<<<nparts, 128, sizeof(TrainSmem), st>>>(P, X, T, dperm, off, B, part, nullptr, nullptr);
     SDF_KERNEL(ctx);
     b1t *= 0.9f;
     b2t *= 0.999f;
     const float lr_t = lr * 0.5f * (1.f + std::cos(3.14159265f * (float)it / (float)steps));  // cosine decay
-    k_adam<<<(kParams + 255) / 256, 256, 0, st>>>(P, G, M1, M2, kParams, lr_t, b1t, b2t);
+    k_train_reduce<<<(kPart + 255) / 256, 256, 0, st>>>(part, nparts, B, P, M1, M2, 1, lr_t, b1t, b2t, nullptr,
+                                                         nullptr);
     SDF_KERNEL(ctx);
   }
   // final loss over the first batch of the shuffle
-  k_gather_batch<<<grid_for(B, 256), 256, 0, st>>>(X, T, dperm, 0, B, XB, TB);
+  k_train_step<<<nparts, 128, sizeof(TrainSmem), st>>>(P, X, T, dperm, 0, B, part, nullptr, nullptr);
   SDF_KERNEL(ctx);
-  k_train_fwd<<<grid_for(B, 128), 128, 0, st>>>(P, XB, TB, B, H0, H1, H2, A3, GY, LS, nullptr);
-  SDF_KERNEL(ctx);
-  k_reduce_loss<<<1, 256, 0, st>>>(LS, B, dl);
+  k_train_reduce<<<(kPart + 255) / 256, 256, 0, st>>>(part, nparts, B, P, nullptr, nullptr, 0, 0.f, 0.f, 0.f, nullptr,
+                                                       dl);
   SDF_KERNEL(ctx);
   __half* WH;
   SDF_TRY(scratch_t(ctx, "mlp_wh", kParams, &WH));

@@ -29,6 +29,10 @@ struct RadiusNorm {
   bool trained = false;
   float alpha = 0.2f;  // radius margin: r = (dhat (1 + alpha) + beta coarse_h / s) s; the
   float beta = 2.0f;   // fastest of the margins measured (it certifies every node on the workloads)
+  // options of the last training (what a SDFGPU_MODE_LEARNED batch trains every mesh with)
+  int train_coarse = 64, train_steps = 400, train_batch = 4096;
+  float train_lr = 3e-3f;
+  uint64_t train_seed = 0;
 };
 
 }  // namespace sdfgpu

@@ -104,6 +104,55 @@ __device__ __forceinline__ bool row_test(const TriRec64& r, double ob, double oc
   return true;
 }
 
+// The decisions of row_test in FP32 with explicit error bands (the bulk of the sign stage's
+// arithmetic).  Returns 0 when the FP64 test certainly misses, 1 when it certainly hits, 2 when a
+// decision lies inside its band (the caller replays row_test in FP64).
+//
+// With (P, Q) the transverse axes in cyclic order after AX, the +AX ray gives h = d x e2 with
+// h_P = -e2_Q, h_Q = e2_P, h_AX = 0, so a = e1_Q e2_P - e1_P e2_Q, s.h = s_Q e2_P - s_P e2_Q and
+// d.q = s_P e1_Q - s_Q e1_P (s_AX = 0).  The six inputs are the FP64 differences the reference
+// forms, rounded once to FP32 (relative error u = 2^-24 each).  A difference of two products of
+// rounded inputs is then within 4u (|p1| + |p2|) of the FP64 value (whose own error, ~2^-51 of the
+// same sum, is far below); 6u is used.  With err_a, err_p those bounds, |A| >= 3 err_a (else the
+// test is undecided) and den = |A| - err_a, the quotient U = fl(P_u / A) satisfies
+//   |u - U| <= E_u = (1.5 err_p + 2 (|U| + 1) err_a) / den + 2u (|U| + 1)
+// (|u| <= 2 (|U| + 1) follows from err_a <= den / 2), the same for v, and
+// |(u + v) - fl(U + V)| <= E_u + E_v + 2u |U + V|.
+constexpr float kU32 = 5.9604645e-8f;  // 2^-24
+
+template <int AX>
+__device__ __forceinline__ int row_test32(const TriRec64& r, double ob, double oc) {
+  constexpr int P = AX == 0 ? 1 : (AX == 1 ? 2 : 0), Q = AX == 0 ? 2 : (AX == 1 ? 0 : 1);
+  // row origin along P and Q (row_test's o: AX = 0 -> (y, z) = (ob, oc); AX = 1 -> (z, x) = (oc, ob);
+  // AX = 2 -> (x, y) = (ob, oc))
+  const double oP = AX == 1 ? oc : ob, oQ = AX == 1 ? ob : oc;
+  const float e1P = (float)ds(r.v[3 + P], r.v[P]), e1Q = (float)ds(r.v[3 + Q], r.v[Q]);
+  const float e2P = (float)ds(r.v[6 + P], r.v[P]), e2Q = (float)ds(r.v[6 + Q], r.v[Q]);
+  const float sP = (float)ds(oP, r.v[P]), sQ = (float)ds(oQ, r.v[Q]);
+  const float a1 = __fmul_rn(e1Q, e2P), a2 = __fmul_rn(e1P, e2Q);
+  const float A = __fsub_rn(a1, a2);
+  const float ea = 6.f * kU32 * (fabsf(a1) + fabsf(a2));
+  const float aA = fabsf(A);
+  if (aA + ea < (float)kEps) return 0;                          // |a| < eps certainly
+  if (!(aA - ea >= (float)kEps) || !(aA >= 3.f * ea)) return 2;  // |a| near eps, or a ill-conditioned
+  const float den = aA - ea;
+  const float u1 = __fmul_rn(sQ, e2P), u2 = __fmul_rn(sP, e2Q);
+  const float U = __fdiv_rn(__fsub_rn(u1, u2), A);
+  const float Eu = (1.5f * 6.f * kU32 * (fabsf(u1) + fabsf(u2)) + 2.f * (fabsf(U) + 1.f) * ea) / den +
+                   2.f * kU32 * (fabsf(U) + 1.f);
+  if (U < -Eu || U > 1.f + Eu) return 0;
+  const float v1 = __fmul_rn(sP, e1Q), v2 = __fmul_rn(sQ, e1P);
+  const float V = __fdiv_rn(__fsub_rn(v1, v2), A);
+  const float Ev = (1.5f * 6.f * kU32 * (fabsf(v1) + fabsf(v2)) + 2.f * (fabsf(V) + 1.f) * ea) / den +
+                   2.f * kU32 * (fabsf(V) + 1.f);
+  if (V < -Ev) return 0;
+  const float UV = __fadd_rn(U, V);
+  const float Euv = Eu + Ev + 2.f * kU32 * fabsf(UV);
+  if (UV > 1.f + Euv) return 0;
+  if (U >= Eu && U <= 1.f - Eu && V >= Ev && UV <= 1.f - Euv) return 1;
+  return 2;
+}
+
 __device__ __forceinline__ bool axis_range2(const GridP& g, int a, double x0, double x1, int64_t& lo, int64_t& hi) {
   const double shift = (double)gidx(g, a, 0);
   double f0 = (x0 - g.o[a]) / g.h - shift - 1e-6, f1 = (x1 - g.o[a]) / g.h - shift + 1e-6;
@@ -120,7 +169,7 @@ __device__ __forceinline__ bool axis_range2(const GridP& g, int a, double x0, do
 template <int AX>
 __device__ __forceinline__ void tri_rows(const GridP& g, const TriRec64& r, bool fill, int64_t row_base,
                                          int32_t* row_cnt, const int32_t* row_off, int32_t* row_cur, RowHit* hits,
-                                         unsigned long long* rkey, int32_t* ridx, int64_t& nhit) {
+                                         unsigned long long* rkey, int32_t* ridx, int64_t& nhit, int64_t& nband) {
   const int b = AX == 0 ? 1 : 0, c = AX == 2 ? 1 : 2;
   int64_t b0, b1, c0, c1;
   if (!axis_range2(g, b, r.bmin[b], r.bmax[b], b0, b1)) return;
@@ -130,11 +179,14 @@ __device__ __forceinline__ void tri_rows(const GridP& g, const TriRec64& r, bool
     for (int64_t jb = b0; jb <= b1; ++jb) {
       const double ob = da(g.o[b], dm(g.h, (double)gidx(g, b, jb)));
       const int64_t row = row_base + jc * g.n[b] + jb;
+      const int dec = row_test32<AX>(r, ob, oc);
+      if (dec == 0) continue;
       if (!fill) {
-        if (row_test<AX>(r, ob, oc, nullptr)) { atomicAdd(&row_cnt[row], 1); ++nhit; }
+        if (dec == 2) ++nband;  // inside the FP32 band: the FP64 test decides
+        if (dec == 1 || row_test<AX>(r, ob, oc, nullptr)) { atomicAdd(&row_cnt[row], 1); ++nhit; }
       } else {
         RowHit R;
-        if (row_test<AX>(r, ob, oc, &R)) {
+        if (row_test<AX>(r, ob, oc, &R)) {  // the hit's FP64 constants (and the band's decision)
           const int32_t pos = row_off[row] + atomicAdd(&row_cur[row], 1);
           hits[pos] = R;
           // sort key: row in the high word, the hit coordinate (ordered float bits) in the low word
@@ -151,16 +203,20 @@ __device__ __forceinline__ void tri_rows(const GridP& g, const TriRec64& r, bool
 __global__ void k_rows(const TriRec64* __restrict__ rec, int64_t nel, GridP g, int64_t base_y, int64_t base_z,
                        bool fill, int32_t* row_cnt, const int32_t* row_off, int32_t* row_cur, RowHit* hits,
                        unsigned long long* rkey, int32_t* ridx, int64_t* counters) {
-  int64_t nhit = 0;
+  int64_t nhit = 0, nband = 0;
   for (int64_t el = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; el < nel; el += (int64_t)gridDim.x * blockDim.x) {
     const TriRec64 r = rec[el];
-    tri_rows<0>(g, r, fill, 0, row_cnt, row_off, row_cur, hits, rkey, ridx, nhit);
-    tri_rows<1>(g, r, fill, base_y, row_cnt, row_off, row_cur, hits, rkey, ridx, nhit);
-    tri_rows<2>(g, r, fill, base_z, row_cnt, row_off, row_cur, hits, rkey, ridx, nhit);
+    tri_rows<0>(g, r, fill, 0, row_cnt, row_off, row_cur, hits, rkey, ridx, nhit, nband);
+    tri_rows<1>(g, r, fill, base_y, row_cnt, row_off, row_cur, hits, rkey, ridx, nhit, nband);
+    tri_rows<2>(g, r, fill, base_z, row_cnt, row_off, row_cur, hits, rkey, ridx, nhit, nband);
   }
   if (!fill) {
-    for (int off = 16; off > 0; off >>= 1) nhit += __shfl_down_sync(0xffffffffu, nhit, off);
+    for (int off = 16; off > 0; off >>= 1) {
+      nhit += __shfl_down_sync(0xffffffffu, nhit, off);
+      nband += __shfl_down_sync(0xffffffffu, nband, off);
+    }
     if ((threadIdx.x & 31) == 0 && nhit) count_add(counters, C_ROW_HITS, nhit);
+    if ((threadIdx.x & 31) == 0 && nband) count_add(counters, C_SIGN_BAND, nband);
   }
 }
 
@@ -355,8 +411,58 @@ __device__ __forceinline__ void child_box2(const BNode& nd, int side, float3& lo
   }
 }
 
+// ray_triangle_intersection (:64-106) for a ray of any direction decided in FP32 with explicit
+// error bands: 0 = the FP64 test certainly misses, 1 = it certainly hits, 2 = a decision lies in
+// its band.  Inputs are the FP64 differences the reference forms (e1, e2, s = o - v1) and the
+// direction, each rounded once to FP32.  Each component of h = d x e2 and q = s x e1 is within
+// 4u of its FP64 value times its absolute-value sum (u = 2^-24), and each three-term dot product
+// over them within 12u times the dot product of the absolute-value sums; the quotients u, v, t
+// then carry the bound of row_test32's comment.  The caller replays mt64 for every hit, certain or
+// not: the hit's t in FP64 is what the reference sorts and de-duplicates within eps.
+__device__ __forceinline__ int mt32(const d3& o, const d3& d, const d3& v1, const d3& v2, const d3& v3) {
+  const float3 e1 = make_float3((float)ds(v2.x, v1.x), (float)ds(v2.y, v1.y), (float)ds(v2.z, v1.z));
+  const float3 e2 = make_float3((float)ds(v3.x, v1.x), (float)ds(v3.y, v1.y), (float)ds(v3.z, v1.z));
+  const float3 sv = make_float3((float)ds(o.x, v1.x), (float)ds(o.y, v1.y), (float)ds(o.z, v1.z));
+  const float3 dv = make_float3((float)d.x, (float)d.y, (float)d.z);
+  // h = d x e2 and the absolute-value sums of its terms
+  const float3 h = make_float3(__fsub_rn(__fmul_rn(dv.y, e2.z), __fmul_rn(dv.z, e2.y)),
+                               __fsub_rn(__fmul_rn(dv.z, e2.x), __fmul_rn(dv.x, e2.z)),
+                               __fsub_rn(__fmul_rn(dv.x, e2.y), __fmul_rn(dv.y, e2.x)));
+  const float3 th = make_float3(fabsf(dv.y * e2.z) + fabsf(dv.z * e2.y), fabsf(dv.z * e2.x) + fabsf(dv.x * e2.z),
+                                fabsf(dv.x * e2.y) + fabsf(dv.y * e2.x));
+  auto dot = [](float3 a, float3 b) { return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z)); };
+  auto adot = [](float3 a, float3 t) { return fabsf(a.x) * t.x + fabsf(a.y) * t.y + fabsf(a.z) * t.z; };
+  const float A = dot(e1, h);
+  const float ea = 12.f * kU32 * adot(e1, th);
+  const float aA = fabsf(A);
+  if (aA + ea < (float)kEps) return 0;
+  if (!(aA - ea >= (float)kEps) || !(aA >= 3.f * ea)) return 2;
+  const float den = aA - ea;
+  auto band = [&](float X, float e) { return (1.5f * e + 2.f * (fabsf(X) + 1.f) * ea) / den + 2.f * kU32 * (fabsf(X) + 1.f); };
+  const float U = __fdiv_rn(dot(sv, h), A);
+  const float Eu = band(U, 12.f * kU32 * adot(sv, th));
+  if (U < -Eu || U > 1.f + Eu) return 0;
+  const float3 q = make_float3(__fsub_rn(__fmul_rn(sv.y, e1.z), __fmul_rn(sv.z, e1.y)),
+                               __fsub_rn(__fmul_rn(sv.z, e1.x), __fmul_rn(sv.x, e1.z)),
+                               __fsub_rn(__fmul_rn(sv.x, e1.y), __fmul_rn(sv.y, e1.x)));
+  const float3 tq = make_float3(fabsf(sv.y * e1.z) + fabsf(sv.z * e1.y), fabsf(sv.z * e1.x) + fabsf(sv.x * e1.z),
+                                fabsf(sv.x * e1.y) + fabsf(sv.y * e1.x));
+  const float V = __fdiv_rn(dot(dv, q), A);
+  const float Ev = band(V, 12.f * kU32 * adot(dv, tq));
+  if (V < -Ev) return 0;
+  const float UV = __fadd_rn(U, V);
+  const float Euv = Eu + Ev + 2.f * kU32 * fabsf(UV);
+  if (UV > 1.f + Euv) return 0;
+  const float T = __fdiv_rn(dot(e2, q), A);
+  const float Et = band(T, 12.f * kU32 * adot(e2, tq));
+  if (T + Et <= (float)kEps) return 0;
+  if (U >= Eu && U <= 1.f - Eu && V >= Ev && UV <= 1.f - Euv && T - Et > (float)kEps) return 1;
+  return 2;
+}
+
 // check_ray_inside_bvh (:114-154) on the LBVH.  Returns parity, or -1 on buffer/stack overflow.
-__device__ int ray_parity(const RayArgs& A, const d3& p, const float3& p32, int dir) {
+// *band counts the ray-triangle tests whose FP32 decision fell in its band.
+__device__ int ray_parity(const RayArgs& A, const d3& p, const float3& p32, int dir, int64_t* band) {
   const d3 d = {c_dirs[3 * dir], c_dirs[3 * dir + 1], c_dirs[3 * dir + 2]};
   const float3 d32 = make_float3((float)d.x, (float)d.y, (float)d.z);
   const float3 inv = make_float3(1.0f / d32.x, 1.0f / d32.y, 1.0f / d32.z);
@@ -377,6 +483,9 @@ __device__ int ray_parity(const RayArgs& A, const d3& p, const float3& p32, int 
       if (!ray_box(p32, d32, inv, lo, hi, A.pad, A.pad)) continue;
       if (ch[side] & kLeafBit) {
         const TriRec64& r = A.rec[A.leaf_prim[ch[side] & 0x7fffffff]];
+        const int dec = mt32(p, d, rec_v(r, 0), rec_v(r, 1), rec_v(r, 2));
+        if (dec == 0) continue;
+        if (dec == 2) ++*band;
         double t;
         if (mt64(p, d, rec_v(r, 0), rec_v(r, 1), rec_v(r, 2), kEps, t)) {
           if (n >= kRayCap) return -1;
@@ -472,7 +581,7 @@ __global__ void k_round(RayArgs A, int64_t nund, int round, int last) {
 __global__ void __launch_bounds__(128) k_rays(RayArgs A, int round) {
   const GridP& g = A.g;
   const int64_t count = A.rq_cnt[round];
-  int64_t rays = 0;
+  int64_t rays = 0, band = 0;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t q = A.req_node[t];
     const int r = A.req_ray[t];
@@ -480,15 +589,19 @@ __global__ void __launch_bounds__(128) k_rays(RayArgs A, int round) {
     const int64_t i = lin % g.n[0], j = (lin / g.n[0]) % g.n[1], k = lin / (g.n[0] * g.n[1]);
     const d3 p = gnode(g, i, j, k);
     const float3 p32 = make_float3((float)(p.x - g.center[0]), (float)(p.y - g.center[1]), (float)(p.z - g.center[2]));
-    int v = ray_parity(A, p, p32, r - 1);
+    int v = ray_parity(A, p, p32, r - 1, &band);
     if (v < 0) { count_add(A.counters, C_ERR_CAPACITY, 1); v = 0; }
     const uint64_t bit = 1ULL << (r - 1);
     if (v) atomicOr((unsigned long long*)&A.parbits[q], (unsigned long long)bit);
     atomicOr((unsigned long long*)&A.have[q], (unsigned long long)bit);
     ++rays;
   }
-  for (int off = 16; off > 0; off >>= 1) rays += __shfl_down_sync(0xffffffffu, rays, off);
+  for (int off = 16; off > 0; off >>= 1) {
+    rays += __shfl_down_sync(0xffffffffu, rays, off);
+    band += __shfl_down_sync(0xffffffffu, band, off);
+  }
   if ((threadIdx.x & 31) == 0 && rays) count_add(A.counters, C_EXTRA_RAYS, rays);
+  if ((threadIdx.x & 31) == 0 && band) count_add(A.counters, C_SIGN_BAND, band);
 }
 
 // generalized_winding_number (:295-328).  The triangles are cut into fixed chunks; one CTA sums

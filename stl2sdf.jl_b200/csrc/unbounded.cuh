@@ -1,0 +1,209 @@
+// unbounded.cuh -- the nearest-triangle search of SDFGPU_MODE_UNBOUNDED shared by the plain
+// packet traversal (k_unbounded, distance.cu) and the learned-radius search (k_learned,
+// learned.cu): the kernel arguments, the per-lane FP32 band of candidate triangles with its FP64
+// resolution in ascending triangle index, and the warp's packet traversal of the LBVH.
+//
+// Both kernels return, for every node, the FP64 minimum over all triangles of the point-triangle
+// distance (tri_step64 without the vertex-skip rule), ties to the lowest triangle index -- the
+// result of folding every triangle in index order (dfOnTriangularMesh.jl:101-177 with the true
+// minimum).  The FP32 search only decides which triangles can hold that minimum.
+#pragma once
+
+#include "common.cuh"
+
+namespace sdfgpu {
+namespace {
+
+constexpr double kBig = 1.0e10;  // abs(-1.0e10), the reference's initial running minimum
+
+__device__ __forceinline__ float3 local32(const GridP& g, const d3& p) {
+  return make_float3((float)(p.x - g.center[0]), (float)(p.y - g.center[1]), (float)(p.z - g.center[2]));
+}
+
+__device__ __forceinline__ void child_box(const BNode& nd, int side, float3& lo, float3& hi) {
+  if (side == 0) {
+    lo = make_float3(nd.a.x, nd.a.y, nd.a.z);
+    hi = make_float3(nd.a.w, nd.b.x, nd.b.y);
+  } else {
+    lo = make_float3(nd.b.z, nd.b.w, nd.c.x);
+    hi = make_float3(nd.c.y, nd.c.z, nd.c.w);
+  }
+}
+
+constexpr int kUnbWarps = 8;     // warps per CTA of k_unbounded
+constexpr int kWarpStack = 64;   // per-warp traversal stack (shared memory)
+constexpr int kKeep = 8;         // per-lane triangles kept inside the FP32 band of the minimum
+
+struct UnbArgs {
+  GridP g;
+  const BNode* nodes;
+  const int32_t* leaf_prim;
+  const float4* v32;
+  const TriRec64* rec;
+  float pad;
+  float eD_abs, eD_rel;
+  int64_t max_visits;
+  const float* radius;  // learned radius per node (nullable)
+  double* dist;
+  double* xp;
+  int64_t* counters;
+  int32_t b[3];         // brick of one warp: nodes along x, y, z (product 32)
+  int64_t nb[3];        // bricks per axis
+  int64_t nbricks;
+};
+
+// The FP64 step out of line: it is rare on this path, and inlining it would size the registers of
+// the whole traversal loop for it.
+__device__ __noinline__ void step64_call(const TriRec64* rec, int prim, const d3& p, double& m64, d3& proj) {
+  tri_step64(rec[prim], p, m64, proj, false);
+}
+
+// Per-lane state of the FP32 search: the smallest FP32 point-triangle distance m (INF before the
+// first hit) and the triangles whose FP32 distance lies within band(m) = m + 2 err(m), one of
+// which is the true (FP64) nearest: |FP32 - FP64| <= err for every distance, so the FP64 winner t*
+// has D32(t*) <= d64(t*) + err <= d64(t_m) + err <= m + 2 err.  The kept triangles live in shared
+// memory (slot q of thread x at q * S + x, S the CTA's thread count: consecutive threads,
+// consecutive banks), which keeps the traversal's registers low.  Free slots hold INF.
+constexpr int kUnbThreads = kUnbWarps * 32;
+struct LaneBest {
+  float m;
+  bool overflow;  // the band held more than kKeep triangles at some point
+  int* t;         // shared: kept triangle ids
+  float* d;       // shared: their FP32 distances
+};
+
+__device__ __forceinline__ float band_of(const UnbArgs& A, float m) { return m + 2.f * (A.eD_abs + A.eD_rel * m); }
+
+template <int S>
+__device__ __forceinline__ void lane_offer(const UnbArgs& A, LaneBest& L, float D, int tri) {
+  if (D < L.m) {
+    L.m = D;
+    const float bd = band_of(A, D);
+#pragma unroll
+    for (int q = 0; q < kKeep; ++q)
+      if (L.d[q * S] > bd) L.d[q * S] = INFINITY;
+  } else if (D > band_of(A, L.m)) {
+    return;
+  }
+  int free_q = -1;
+  bool dup = false;
+#pragma unroll
+  for (int q = 0; q < kKeep; ++q) {
+    const float dq = L.d[q * S];
+    if (dq != INFINITY && L.t[q * S] == tri) dup = true;  // already kept (a second pass)
+    if (free_q < 0 && dq == INFINITY) free_q = q;
+  }
+  if (dup) return;
+  if (free_q < 0) {
+    L.overflow = true;
+    return;
+  }
+  L.d[free_q * S] = D;
+  L.t[free_q * S] = tri;
+}
+
+// One warp searches the LBVH for the nearest triangles of its 32 nodes together (a packet
+// traversal).  The stack is the warp's, in shared memory; a child is visited when its box lies
+// within the bound of at least one active lane -- band(m) of the lane's FP32 minimum, or r0 before
+// its first hit -- nearer child first as seen from the brick's central lane `rep`.  Every load of
+// a node or triangle is the same address for the whole warp.  kExact: every leaf triangle within a
+// lane's bound runs the FP64 step at once (used with a tight r0 for lanes whose band overflowed);
+// otherwise leaves only feed the lane's FP32 band.  Returns false when the visit or stack bound is
+// exceeded.
+template <bool kExact, int S>
+__device__ bool warp_search(const UnbArgs& A, int* stack, int lane, int rep, const d3& p, const float3& p32,
+                            bool active, float r0, LaneBest& L, double& m64, d3& proj, int64_t& fp64,
+                            int64_t& visits_out) {
+  int sp = 1;
+  if (lane == 0) stack[0] = 0;
+  __syncwarp();
+  int64_t visits = 0;
+  bool ok = true;
+  while (sp > 0) {
+    if (++visits > A.max_visits) { ok = false; break; }
+    const int nid = stack[--sp];
+    __syncwarp();
+    const BNode nd = A.nodes[nid];
+    float3 lo0, hi0, lo1, hi1;
+    child_box(nd, 0, lo0, hi0);
+    child_box(nd, 1, lo1, hi1);
+    const bool e0 = lo0.x > hi0.x, e1 = lo1.x > hi1.x;  // empty child
+    const float d0 = box_d2(p32, lo0, hi0), d1 = box_d2(p32, lo1, hi1);
+    float lim;
+    if (kExact) {
+      const float mf = (float)m64;
+      lim = fminf(r0, mf + A.eD_abs + A.eD_rel * mf);
+    } else {
+      lim = L.m < INFINITY ? band_of(A, L.m) : r0 + A.eD_abs + A.eD_rel * r0;
+    }
+    const float b = lim + A.pad;
+    const float b2 = b * b;
+    const bool w0 = active && !e0 && d0 <= b2, w1 = active && !e1 && d1 <= b2;
+    const unsigned m0 = __ballot_sync(0xffffffffu, w0), m1 = __ballot_sync(0xffffffffu, w1);
+    const float rd0 = __shfl_sync(0xffffffffu, e0 ? INFINITY : d0, rep);
+    const float rd1 = __shfl_sync(0xffffffffu, e1 ? INFINITY : d1, rep);
+    const bool swap = rd1 < rd0;
+    const int cn = swap ? nd.d.y : nd.d.x, cf = swap ? nd.d.x : nd.d.y;
+    const unsigned mn = swap ? m1 : m0, mfar = swap ? m0 : m1;
+    const bool wn = swap ? w1 : w0, wf = swap ? w0 : w1;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {  // leaves now, near one first
+      const int c = q == 0 ? cn : cf;
+      const bool want = q == 0 ? wn : wf;
+      if (!(c & kLeafBit) || (q == 0 ? mn : mfar) == 0u) continue;
+      const int prim = A.leaf_prim[c & 0x7fffffff];
+      const float D = sqrtf(pt_tri_d2(p32, f3(A.v32[3 * prim]), f3(A.v32[3 * prim + 1]), f3(A.v32[3 * prim + 2])));
+      if (kExact) {
+        const float mf = (float)m64;
+        if (want && D <= fminf(r0, mf + A.eD_abs + A.eD_rel * mf)) {
+          step64_call(A.rec, prim, p, m64, proj);
+          ++fp64;
+        }
+      } else {
+        const float limq = L.m < INFINITY ? band_of(A, L.m) : r0 + A.eD_abs + A.eD_rel * r0;
+        if (want && D <= limq) lane_offer<S>(A, L, D, prim);
+      }
+    }
+    // inner children, the far one pushed first so the near one is popped next
+    if (mfar != 0u && !(cf & kLeafBit)) {
+      if (sp >= kWarpStack) { ok = false; break; }
+      if (lane == 0) stack[sp] = cf;
+      ++sp;
+    }
+    if (mn != 0u && !(cn & kLeafBit)) {
+      if (sp >= kWarpStack) { ok = false; break; }
+      if (lane == 0) stack[sp] = cn;
+      ++sp;
+    }
+    __syncwarp();
+  }
+  __syncwarp();
+  visits_out += visits;
+  return ok;
+}
+
+// FP64 steps over the kept triangles inside the final band, in ascending triangle index (so exact
+// ties keep the lowest index, as a fold in index order does).
+template <int S>
+__device__ __forceinline__ void lane_resolve(const UnbArgs& A, const LaneBest& L, const d3& p, double& m64, d3& proj,
+                                             int64_t& fp64) {
+  const float bd = band_of(A, L.m);
+  int last = -1;
+#pragma unroll 1
+  for (int it = 0; it < kKeep; ++it) {
+    int best = 0x7fffffff;
+#pragma unroll
+    for (int q = 0; q < kKeep; ++q) {
+      const int tq = L.t[q * S];
+      if (L.d[q * S] <= bd && tq > last && tq < best) best = tq;
+    }
+    if (best == 0x7fffffff) break;
+    step64_call(A.rec, best, p, m64, proj);
+    ++fp64;
+    last = best;
+  }
+}
+
+
+}  // namespace
+}  // namespace sdfgpu

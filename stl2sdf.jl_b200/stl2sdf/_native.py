@@ -51,6 +51,7 @@ class Stats(ctypes.Structure):
         ("ms_fold", ctypes.c_double), ("ms_rows", ctypes.c_double), ("ms_parity", ctypes.c_double),
         ("ms_vote", ctypes.c_double), ("certified_nodes", ctypes.c_int64), ("radius_loss", ctypes.c_double),
         ("bvh_visits", ctypes.c_int64), ("ms_train", ctypes.c_double), ("train_launches", ctypes.c_int64),
+        ("sign_band_reruns", ctypes.c_int64),
     ]
 
     def as_dict(self):

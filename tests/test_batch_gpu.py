@@ -155,3 +155,27 @@ def test_workload_batch_items_match_oracle(gpu_ctx):
             r = oracle.signs(X, IEN, o, h, N, nodes=nodes)
             assert np.array_equal(dist[nodes], d_ref)
             assert np.array_equal(sign[nodes], r["sign"]) and np.array_equal(conf[nodes], r["conf"])
+
+
+def test_learned_batch_equals_unbounded_and_oracle(gpu_ctx, small_batch):
+    """SDFGPU_MODE_LEARNED over the uneven batch: every mesh trains its own radius network inside
+    the call; the fields equal the plain unbounded batch bit for bit, and sampled nodes of three
+    meshes equal the oracle's unbounded distance and its sign."""
+    from stl2sdf import _native
+
+    plain = gpu_ctx.sdf_batch(small_batch, mode=_native.MODE_UNBOUNDED, streams=4, autotune=True, want_parts=True)
+    learned = gpu_ctx.sdf_batch(small_batch, mode=_native.MODE_LEARNED, streams=4, autotune=True, want_parts=True)
+    st = gpu_ctx.stats()
+    assert st["certified_nodes"] + st["unbounded_fallbacks"] == st["ngp"]
+    assert st["train_launches"] > 0 and st["ms_train"] > 0
+    for a, b in zip(learned, plain):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    picks = sorted(range(len(small_batch)), key=lambda k: small_batch[k][1].shape[0])[:3]
+    for k in picks:
+        X, IEN, o, h, N = small_batch[k]
+        sdf, dist, sign, conf = learned[k]
+        nodes = sample_nodes(sdf.shape[0], 800, seed=5)
+        d_ref, _, _ = oracle.distances(X, IEN, o, h, N, mode=2, nodes=nodes)
+        assert np.array_equal(dist[nodes], d_ref)
+        assert np.array_equal(sign[nodes], oracle.signs(X, IEN, o, h, N, nodes=nodes)["sign"])

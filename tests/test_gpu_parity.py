@@ -263,49 +263,6 @@ def test_gyroid_small_full(gpu_ctx):
     assert st["undecided_nodes"] == int(np.count_nonzero(ref["rays"] > 6))
 
 
-def test_blobs_full_size_sample(gpu_ctx):
-    """Workload 3 mesh (64 blobs at 512^3, ~1.4M triangles) on its 256-node grid: every node on the
-    GPU, a seeded sample of 3,000 nodes in the oracle; plus size-independent properties."""
-    from stl2sdf import DataImport
-    from workloads import synthetic
-
-    V, F = synthetic.blobs(64, seed=2, cells=512)
-    X, IEN = DataImport.roundtrip_float32(V, F)
-    g = grid_of(X, n_nodes_long_axis=256)
-    gpu_ctx.set_mesh(X, IEN)
-    sdf, dist, sign, conf = gpu_ctx.sdf(g["origin"], g["h"], g["N"], want_parts=True)
-    assert np.all((dist >= 0) & (dist <= g["h"]))
-    assert np.all(np.abs(sign) == 1.0) and np.array_equal(sdf, dist * sign)
-    nodes = sample_nodes(g["ngp"], 3000, seed=11)
-    dr, _, _ = oracle.distances(X, IEN, g["origin"], g["h"], g["N"], mode=0, nodes=nodes)
-    check_dist(dist[nodes], dr, X)
-    ref = oracle.signs(X, IEN, g["origin"], g["h"], g["N"], nodes=nodes)
-    assert np.array_equal(sign[nodes], ref["sign"]) and np.array_equal(conf[nodes], ref["conf"])
-
-
-def test_gyroid_full_size_sample(gpu_ctx):
-    """Workload 5 mesh (gyroid sheet at 384^3, ~5.7M triangles) on its 320-node grid: every node on
-    the GPU; in the oracle 1,500 seeded uniform nodes plus 1,500 seeded nodes within one cell of the
-    sheet (where grazing axis rays, edge/vertex hits and near-equidistant triangles are)."""
-    from stl2sdf import DataImport
-    from workloads import synthetic
-
-    V, F = synthetic.gyroid(384, 0.04, 2.0)
-    X, IEN = DataImport.roundtrip_float32(V, F)
-    g = grid_of(X, n_nodes_long_axis=320)
-    gpu_ctx.set_mesh(X, IEN)
-    sdf, dist, sign, conf = gpu_ctx.sdf(g["origin"], g["h"], g["N"], want_parts=True)
-    assert np.array_equal(sdf, dist * sign)
-    rng = np.random.default_rng(17)
-    near = np.flatnonzero(dist < g["h"])
-    nodes = np.unique(np.concatenate([sample_nodes(g["ngp"], 1500, seed=17),
-                                      rng.choice(near, size=min(1500, near.size), replace=False)])).astype(np.int64)
-    dr, _, _ = oracle.distances(X, IEN, g["origin"], g["h"], g["N"], mode=0, nodes=nodes)
-    check_dist(dist[nodes], dr, X)
-    ref = oracle.signs(X, IEN, g["origin"], g["h"], g["N"], nodes=nodes)
-    assert np.array_equal(sign[nodes], ref["sign"]) and np.array_equal(conf[nodes], ref["conf"])
-
-
 def _bipyramid(k=24):
     """Closed double fan: two apexes shared by k triangles each (a vertex far above the number of
     triangles the unbounded search keeps per node in its FP32 band, so nodes on the axis take

@@ -96,6 +96,79 @@ def test_vti_roundtrip(tmp_path):
         DataExport.exportSdfToVTI(str(tmp_path / "bad"), g, vals[:-1], "distance")
 
 
+def _decode_vti_from_spec(path):
+    """A decoder written from the VTK XML file-format description, independent of DataExport:
+    the XML header is parsed as XML (the raw appended block cut out), and the appended data is
+    decoded by its rules -- an '_' marker, then at the array's offset either a UInt64 byte count and
+    the raw bytes, or (vtkZLibDataCompressor) a UInt64 header [number of blocks, uncompressed block
+    size, uncompressed size of the last block (0: a full block), compressed size of each block]
+    followed by the zlib streams."""
+    import struct
+    import xml.etree.ElementTree as ET
+    import zlib
+
+    data = open(path, "rb").read()
+    a = data.index(b"<AppendedData")
+    marker = data.index(b"_", a) + 1
+    end = data.rindex(b"</AppendedData>")
+    root = ET.fromstring(data[:marker - 1] + data[end:])
+    assert root.tag == "VTKFile" and root.get("type") == "ImageData"
+    assert root.get("byte_order") == "LittleEndian" and root.get("header_type") == "UInt64"
+    img = root.find("ImageData")
+    ext = [int(v) for v in img.get("WholeExtent").split()]
+    assert img.find("Piece").get("Extent") == img.get("WholeExtent")
+    arr = img.find("Piece").find("PointData").find("DataArray")
+    assert arr.get("format") == "appended" and root.find("AppendedData").get("encoding") == "raw"
+    size = {"Float64": 8, "Float32": 4}[arr.get("type")]
+    blob = data[marker + int(arr.get("offset")):]
+    if root.get("compressor") == "vtkZLibDataCompressor":
+        nb, bs, last = struct.unpack("<3Q", blob[:24])
+        csz = struct.unpack(f"<{nb}Q", blob[24:24 + 8 * nb])
+        pos, raw = 24 + 8 * nb, b""
+        for q in range(nb):
+            part = zlib.decompress(blob[pos:pos + csz[q]])
+            want = (last if last else bs) if q == nb - 1 else bs
+            assert len(part) == want
+            raw += part
+            pos += csz[q]
+    else:
+        assert root.get("compressor") is None
+        (n,) = struct.unpack("<Q", blob[:8])
+        raw = blob[8:8 + n]
+    dims = [ext[1] - ext[0] + 1, ext[3] - ext[2] + 1, ext[5] - ext[4] + 1]
+    assert len(raw) == size * dims[0] * dims[1] * dims[2]
+    vals = np.frombuffer(raw, dtype="<f8" if size == 8 else "<f4")
+    return (vals, dims, [float(v) for v in img.get("Origin").split()], [float(v) for v in img.get("Spacing").split()],
+            arr.get("Name"), img.get("Direction"))
+
+
+def test_vti_layout_by_an_independent_decoder(tmp_path):
+    """The writer's files decoded by the spec-based decoder above: uncompressed, one zlib block,
+    several zlib blocks (a field over 4 MiB), Float64 and the Float32 smoothed field, values x
+    fastest (ExportToVTI.jl:55-64 reshapes the field to N+1 per axis, x first)."""
+    from stl2sdf import DataExport, MeshGrid
+
+    rng = np.random.default_rng(4)
+    for hi, n_max, comp, smooth in (((1.0, 0.5, 2.25), 8, False, None), ((1.0, 0.5, 2.25), 8, True, None),
+                                    ((1.0, 2.0, 4.0), 74, True, None), ((1.0, 0.5, 2.25), 8, True, 2)):
+        g = MeshGrid.Grid([-1.0, 0.0, 2.0], list(hi), n_max, 3)
+        dims = (g.N + 1) if smooth is None else g.N * smooth + 1
+        n = int(np.prod(dims))
+        vals = rng.normal(size=n).astype(np.float32 if smooth else np.float64)
+        path = DataExport.exportSdfToVTI(str(tmp_path / f"f{n_max}{comp}{smooth}"), g, vals, "distance",
+                                         smooth=smooth, compress=comp)
+        got, gdims, origin, spacing, label, direction = _decode_vti_from_spec(path)
+        assert np.array_equal(got, vals) and gdims == [int(v) for v in dims]
+        assert origin == [float(v) for v in g.AABB_min]
+        h = g.cell_size / (smooth or 1)
+        assert spacing == [h, h, h] and label == "distance" and direction == "1 0 0 0 1 0 0 0 1"
+        # x fastest: the value at (i, j, k) sits at i + nx (j + ny k)
+        i, j, k = dims[0] - 1, 1, 1
+        assert got[i + dims[0] * (j + dims[1] * k)] == vals.reshape(dims[2], dims[1], dims[0])[k, j, i]
+        if n_max == 74:  # this field spans more than one 4 MiB zlib block
+            assert 8 * n > (1 << 22)
+
+
 def test_workload_meshes():
     from workloads import synthetic
 

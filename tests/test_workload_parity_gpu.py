@@ -1,0 +1,127 @@
+"""Parity on the two largest workload meshes at their full grid sizes, where the headline runs:
+the 64-blob marching-cubes mesh (~1.4M triangles, 256 nodes on the long axis) and the capped
+gyroid sheet (~5.7M triangles, 320 nodes on the long axis).
+
+Every node is computed on the GPU; the oracle checks seeded samples -- uniform nodes plus a large
+sample of nodes within one cell of the surface, where the candidate sets, the vertex-skip rule,
+grazing axis rays and near-equidistant triangles are -- in the reference rule (distance and sign),
+in the plain unbounded search and in the learned-radius search.  Size-independent properties are
+checked on the whole grid: 0 <= d <= h in the reference rule, |sign| = 1, sdf = dist * sign,
+the learned search equal to the plain search at every node, and the unbounded distance never above
+the clamped one.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import grid_of, sample_nodes
+
+pytestmark = pytest.mark.gpu
+
+DIST_TOL_DIAG = 1e-6  # |d| error bar relative to the bounding-box diagonal (bit-exactness is asserted too)
+TRAIN = dict(coarse_n=64, steps=400, batch=4096, lr=3e-3, seed=0)  # the bench's per-mesh training
+
+
+def _mesh(name):
+    import workloads
+    from stl2sdf import DataImport
+
+    X, IEN = DataImport.roundtrip_float32(*workloads.mesh(name))
+    kind, v = workloads.grid_args(name)
+    return X, IEN, grid_of(X, n_nodes_long_axis=v + 7)
+
+
+@pytest.fixture(scope="module")
+def blobs256():
+    return _mesh("blobs256")
+
+
+@pytest.fixture(scope="module")
+def gyroid320():
+    return _mesh("gyroid320")
+
+
+def _exact(got, want, X):
+    diag = float(np.linalg.norm(X.max(0) - X.min(0)))
+    assert np.abs(got - want).max() <= DIST_TOL_DIAG * diag
+    bad = np.flatnonzero(got != want)
+    assert bad.size == 0, f"{bad.size} values differ, first at {bad[:5]}: {got[bad[:5]]} vs {want[bad[:5]]}"
+
+
+def _ref_rule(ctx, X, IEN, g, n_uniform, n_near, seed):
+    ctx.set_mesh(X, IEN)
+    sdf, dist, sign, conf = ctx.sdf(g["origin"], g["h"], g["N"], want_parts=True)
+    assert np.all((dist >= 0) & (dist <= g["h"]))
+    assert np.all(np.abs(sign) == 1.0) and np.array_equal(sdf, dist * sign)
+    near = np.flatnonzero(dist < g["h"])
+    rng = np.random.default_rng(seed)
+    picks = rng.choice(near, size=min(n_near, near.size), replace=False)
+    nodes = np.unique(np.concatenate([sample_nodes(g["ngp"], n_uniform, seed=seed), picks])).astype(np.int64)
+    dr, _, _ = oracle.distances(X, IEN, g["origin"], g["h"], g["N"], mode=0, nodes=nodes)
+    _exact(dist[nodes], dr, X)
+    ref = oracle.signs(X, IEN, g["origin"], g["h"], g["N"], nodes=nodes)
+    assert np.array_equal(sign[nodes], ref["sign"]) and np.array_equal(conf[nodes], ref["conf"])
+    return dist, sign, nodes.size
+
+
+def _unbounded_and_learned(ctx, X, IEN, g, clamped, n_uniform, n_near, seed):
+    ctx.set_mesh(X, IEN)
+    plain, _ = ctx.distances(g["origin"], g["h"], g["N"], 2)
+    ms_plain = ctx.stats()["ms_distance"]
+    ctx.train_radius(**TRAIN)
+    ms_train = ctx.stats()["ms_train"]
+    learned, _ = ctx.distances(g["origin"], g["h"], g["N"], 3)
+    st = ctx.stats()
+    assert np.array_equal(plain, learned), "learned-radius search differs from the plain search"
+    assert st["certified_nodes"] + st["unbounded_fallbacks"] == g["ngp"]
+    assert np.all(np.minimum(plain, g["h"]) <= clamped)  # the clamped modes never go below the true minimum
+    near = np.flatnonzero(plain < 2 * g["h"])
+    rng = np.random.default_rng(seed)
+    nodes = np.unique(np.concatenate([sample_nodes(g["ngp"], n_uniform, seed=seed),
+                                      rng.choice(near, size=min(n_near, near.size), replace=False)])).astype(np.int64)
+    dr, _, _ = oracle.distances(X, IEN, g["origin"], g["h"], g["N"], mode=2, nodes=nodes)
+    _exact(learned[nodes], dr, X)
+    return ms_plain, st["ms_distance"], ms_train, st["certified_nodes"] / g["ngp"]
+
+
+def test_blobs256_reference_rule_near_surface(gpu_ctx, blobs256):
+    """Reference rule on the 256-node grid of the blob mesh: 3,000 uniform nodes and 20,000 nodes
+    within one cell of the surface against the oracle (distance bit-exact, sign and confidence
+    equal)."""
+    X, IEN, g = blobs256
+    _, _, n = _ref_rule(gpu_ctx, X, IEN, g, 3000, 20000, seed=11)
+    assert n >= 20000
+
+
+def test_blobs256_unbounded_and_learned(gpu_ctx, blobs256):
+    """Plain unbounded and learned-radius searches on the full 256-node grid: identical at every
+    node, equal to the oracle on 2,000 uniform and 2,000 near-surface nodes; the trained network
+    certifies most nodes and its search (training included) beats the plain one."""
+    X, IEN, g = blobs256
+    gpu_ctx.set_mesh(X, IEN)
+    clamped, _ = gpu_ctx.distances(g["origin"], g["h"], g["N"], 1)
+    ms_plain, ms_learned, ms_train, cert = _unbounded_and_learned(gpu_ctx, X, IEN, g, clamped, 2000, 2000, seed=13)
+    print(f"blobs256: plain {ms_plain:.2f} ms, learned {ms_learned:.2f} ms + training {ms_train:.2f} ms, "
+          f"certified {cert:.4f}")
+    assert cert >= 0.9
+    assert ms_learned + ms_train < ms_plain
+
+
+def test_gyroid320_reference_rule_near_surface(gpu_ctx, gyroid320):
+    """Reference rule on the 320-node grid of the gyroid sheet: 1,500 uniform and 5,000
+    near-surface nodes (grazing axis rays, edge/vertex hits, near-equidistant triangles)."""
+    X, IEN, g = gyroid320
+    _ref_rule(gpu_ctx, X, IEN, g, 1500, 5000, seed=17)
+
+
+def test_gyroid320_unbounded_and_learned(gpu_ctx, gyroid320):
+    X, IEN, g = gyroid320
+    gpu_ctx.set_mesh(X, IEN)
+    clamped, _ = gpu_ctx.distances(g["origin"], g["h"], g["N"], 1)
+    ms_plain, ms_learned, ms_train, cert = _unbounded_and_learned(gpu_ctx, X, IEN, g, clamped, 1000, 1000, seed=19)
+    print(f"gyroid320: plain {ms_plain:.2f} ms, learned {ms_learned:.2f} ms + training {ms_train:.2f} ms, "
+          f"certified {cert:.4f}")
+    assert cert >= 0.9
