@@ -41,7 +41,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "SDF grid nodes/s on 1 B200: learned-radius vs plain GPU vs CPU ref, sign exact"
 L2_NOTE = "a 256 MB device write between timed steps flushes the 126 MB L2 (the mesh records and fields exceed it too)"
-TRAIN = dict(coarse_n=64, steps=400, batch=4096, lr=3e-3, seed=0)  # the learned form's per-mesh training
+TRAIN = dict(coarse_n=32, steps=200, batch=2048, lr=5e-3, seed=0)  # the learned form's per-mesh training
 
 
 def common_config(name, X, IEN, g):
@@ -480,9 +480,14 @@ def distance_variants(ctx, X, IEN, g, reps=3, work=None, peak_tflops=None):
                                      "fallback_nodes": st["unbounded_fallbacks"],
                                      "fallback_rate": st["unbounded_fallbacks"] / g["ngp"], "train_ms": train_ms,
                                      "train_loss": st["radius_loss"], "train": dict(TRAIN)})
+    # the same search with every radius infinite: what the network's bound adds
+    ctx.set_radius_margin(float("inf"), 0.0)
+    out["learned_search_without_network"] = run(2, learned=True)
+    ctx.set_radius_margin()
     lu = out["learned_unbounded"]
     lu["ms_with_training"] = lu["ms"] + train_ms
     out["learned_vs_plain_unbounded"] = out["plain_unbounded"]["ms"] / lu["ms"]
+    out["network_gain"] = out["learned_search_without_network"]["ms"] / lu["ms"]
     out["learned_with_training_vs_plain_unbounded"] = out["plain_unbounded"]["ms"] / lu["ms_with_training"]
     if work is not None and peak_tflops:
         # FP32 roofline of the distance stage alone: F_pt |D*| per node (clamped forms) or F_pt |D*_u|

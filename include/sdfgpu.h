@@ -245,8 +245,8 @@ int sdfgpu_sdf_batch(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count, i
  * workers by a fixed longest-processing-time assignment, so repeated batches reuse their buffers.
  * Unbounded and learned-radius batches always run per item.  With mode = SDFGPU_MODE_LEARNED
  * every mesh gets its own radius network, trained right after its LBVH with the options of the last
- * sdfgpu_train_radius on ctx (defaults: 400 steps, batch 4096, learning rate 3e-3, seed 0) on a
- * coarse grid of min(64, K / 2) nodes on its longest axis (at least 16), K the nodes on the longest
+ * sdfgpu_train_radius on ctx (defaults: 200 steps, batch 2048, learning rate 5e-3, seed 0) on a
+ * coarse grid of min(32, K / 2) nodes on its longest axis (at least 16), K the nodes on the longest
  * axis of the mesh's own grid; results equal SDFGPU_MODE_UNBOUNDED. */
 int sdfgpu_sdf_batch_ex(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count, int32_t mode, int32_t min_rays,
                         int32_t max_rays, double confidence_threshold, int32_t use_winding_fallback, int32_t streams,
@@ -265,7 +265,7 @@ int sdfgpu_autotune(sdfgpu_ctx* ctx, const double origin[3], double h, const int
 /* Learned search radius for SDFGPU_MODE_UNBOUNDED (an extension of the reference's distance
  * search; no reference counterpart).  A 3 x 64 Fourier-feature MLP (FP16 weights, FP32
  * accumulate) is trained on the GPU on the exact unbounded distances of a coarse grid of the current
- * mesh (coarse_n nodes on its longest axis, Grid(Xmin, Xmax, coarse_n - 7, 3)).  sdfgpu_distances
+ * mesh (coarse_n - 1 cells on the longest axis of the mesh box, padded by one cell).  sdfgpu_distances
  * with use_learned_radius = 1 then bounds each node's search by the predicted radius; a hit inside
  * it is certified exact, other nodes fall back to the unbounded search (stats: certified_nodes,
  * unbounded_fallbacks).  Results are bit-identical to the plain unbounded mode. */
@@ -275,8 +275,10 @@ int sdfgpu_train_radius(sdfgpu_ctx* ctx, int32_t coarse_n, int32_t steps, int32_
  * product 32) whose nearest triangles one warp searches together.  Default 4 x 2 x 4. */
 int sdfgpu_set_brick(sdfgpu_ctx* ctx, const int32_t brick[3]);
 /* Margin of the learned radius: r = (dhat (1 + alpha) + beta * coarse spacing / s) * s, where dhat is
- * the network's normalised distance and s its normalisation scale.  Defaults alpha = 0.2, beta = 2.
- * A smaller margin prunes more and certifies fewer nodes; results never change. */
+ * the network's normalised distance and s its normalisation scale.  Defaults alpha = 0.5, beta = 4.
+ * A smaller margin prunes more and certifies fewer nodes; results never change.  alpha = +inf makes
+ * every radius infinite: the learned mode's search without the network's bound (to measure what the
+ * network gains). */
 int sdfgpu_set_radius_margin(sdfgpu_ctx* ctx, float alpha, float beta);
 /* Number of FP32 parameters of the radius network (layout: W1 64x32, b1, W2 64x64, b2, W3 64x64,
  * b3, w4 64, b4). */

@@ -609,8 +609,9 @@ int sdfgpu_set_radius_params(sdfgpu_ctx* ctx, const float* params, const double 
 
 int sdfgpu_set_radius_margin(sdfgpu_ctx* ctx, float alpha, float beta) {
   SDF_TRY(begin_call(ctx));
-  if (!(alpha >= 0.f && alpha <= 10.f) || !(beta >= 0.f && beta <= 100.f))
-    return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "radius margin: need 0 <= alpha <= 10 and 0 <= beta <= 100");
+  if (!((alpha >= 0.f && alpha <= 10.f) || std::isinf(alpha) && alpha > 0.f) || !(beta >= 0.f && beta <= 100.f))
+    return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT,
+                "radius margin: need 0 <= alpha <= 10 (or +inf: no bound) and 0 <= beta <= 100");
   ctx->radius.alpha = alpha;
   ctx->radius.beta = beta;
   return SDFGPU_OK;

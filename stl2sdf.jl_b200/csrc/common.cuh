@@ -224,6 +224,8 @@ int ensure_ine(sdfgpu_ctx* ctx);
 int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, double* d_dist, double* d_xp);
 // The learned-radius nearest-triangle search (learned.cu) with one FP32 radius per node.
 int run_learned(sdfgpu_ctx* ctx, const GridP& g, const float* radius, double* d_dist, double* d_xp);
+// Exact unbounded distances of a sparse grid's nodes, one thread per node (learned.cu).
+int run_nearest_points(sdfgpu_ctx* ctx, const GridP& g, double* d_dist);
 
 // The reference-rule / h-bounded distance stage in parts (distance.cu), so a batch can run the folds
 // of many meshes in one launch: dist_prepare builds one mesh's tile lists and fold arguments,

@@ -29,6 +29,8 @@
 #include <cub/cub.cuh>
 #include <cuda_fp16.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "common.cuh"
@@ -503,8 +505,7 @@ __global__ void __launch_bounds__(kUnbThreads, 3) k_unbounded(UnbArgs A) {
   const int lx = lane % A.b[0], ly = (lane / A.b[0]) % A.b[1], lz = lane / (A.b[0] * A.b[1]);
   const int rep = A.b[0] / 2 + A.b[0] * (A.b[1] / 2 + A.b[1] * (A.b[2] / 2));
   int64_t fp64 = 0, cert = 0, fallback = 0, errs = 0, visits = 0;
-  for (int64_t brick = (int64_t)blockIdx.x * kUnbWarps + w; brick < A.nbricks;
-       brick += (int64_t)gridDim.x * kUnbWarps) {
+  for (int64_t brick = next_brick(A, lane); brick < A.nbricks; brick = next_brick(A, lane)) {
     const int64_t bx = brick % A.nb[0], by = (brick / A.nb[0]) % A.nb[1], bz = brick / (A.nb[0] * A.nb[1]);
     const int64_t i = bx * A.b[0] + lx, j = by * A.b[1] + ly, k = bz * A.b[2] + lz;
     const bool valid = i <= g.N[0] && j <= g.N[1] && k <= g.N[2];
@@ -596,9 +597,12 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
     if (use_learned) {
       // r = (dhat (1 + alpha) + beta * coarse spacing / s) s: a margin for the network's error and
       // for the interpolation between the training nodes
-      SDF_TRY(scratch_t(ctx, "radius", (size_t)g.ngp, &radius));
+      // (alpha = +inf: every radius infinite, the same search without the network's bound)
       const RadiusNorm& R = ctx->radius;
-      SDF_TRY(run_radius(ctx, &g, nullptr, g.ngp, R.alpha, (float)(R.beta * R.coarse_h / R.s), radius));
+      if (!std::isinf(R.alpha)) {
+        SDF_TRY(scratch_t(ctx, "radius", (size_t)g.ngp, &radius));
+        SDF_TRY(run_radius(ctx, &g, nullptr, g.ngp, R.alpha, (float)(R.beta * R.coarse_h / R.s), radius));
+      }
       SDF_MARK(ctx, T_TILES);
       SDF_TRY(run_learned(ctx, g, radius, d_dist, d_xp));
       SDF_MARK(ctx, T_FOLD);
@@ -612,7 +616,13 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
       A.nbricks *= A.nb[a];
     }
     SDF_MARK(ctx, T_TILES);
-    k_unbounded<<<grid_for(A.nbricks, kUnbWarps, 148 * 8), kUnbWarps * 32, 0, st>>>(A);
+    // one resident wave of CTAs draining the brick queue
+    SDF_TRY(scratch_t(ctx, "brick_next", 1, &A.next));
+    SDF_CUDA(ctx, cudaMemsetAsync(A.next, 0, sizeof(unsigned long long), st));
+    int per_sm = 0, sms = 148;
+    SDF_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_unbounded, kUnbWarps * 32, 0));
+    SDF_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    k_unbounded<<<grid_for(A.nbricks, kUnbWarps, (int64_t)sms * std::max(per_sm, 1)), kUnbWarps * 32, 0, st>>>(A);
     SDF_KERNEL(ctx);
     SDF_MARK(ctx, T_FOLD);
     return 0;

@@ -11,7 +11,11 @@
 // contiguous runs of the Morton-sorted leaves, whose FP32 vertices and boxes are stored in leaf
 // order, see k_leaf_order in mesh.cu).  Each lane then tests the gathered clusters against its own
 // bound and folds the triangles of the clusters it needs, all lanes in step.  As lanes find
-// triangles their bounds shrink to band(m) and the brick bound R shrinks with them.
+// triangles their bounds shrink to band(m) and the brick bound R shrinks with them.  Before the
+// expansion every brick takes one greedy nearest-first descent to a cluster near its centre and
+// folds it on every lane, so the lanes' bounds are close to their distances from the start.  With no
+// radius array every bound is infinite and the search rests on that seed alone (the coarse grid the
+// network trains on is computed this way, and it measures what the network adds).
 //
 // Certification (the same rule as the plain search seeded with r): a lane whose FP32 minimum m
 // satisfies m + err(m) <= r has its FP64 nearest triangle within r, and every triangle within r
@@ -77,7 +81,7 @@ __global__ void __launch_bounds__(kLThreads) k_learned(LearnArgs LA) {
   const int lx = lane % A.b[0], ly = (lane / A.b[0]) % A.b[1], lz = lane / (A.b[0] * A.b[1]);
   const int rep = A.b[0] / 2 + A.b[0] * (A.b[1] / 2 + A.b[1] * (A.b[2] / 2));
   int64_t fp64 = 0, cert = 0, fallback = 0, errs = 0, visits = 0;
-  for (int64_t brick = (int64_t)blockIdx.x * kLWarps + w; brick < A.nbricks; brick += (int64_t)gridDim.x * kLWarps) {
+  for (int64_t brick = next_brick(A, lane); brick < A.nbricks; brick = next_brick(A, lane)) {
     const int64_t bx = brick % A.nb[0], by = (brick / A.nb[0]) % A.nb[1], bz = brick / (A.nb[0] * A.nb[1]);
     const int64_t i = bx * A.b[0] + lx, j = by * A.b[1] + ly, k = bz * A.b[2] + lz;
     const bool valid = i <= g.N[0] && j <= g.N[1] && k <= g.N[2];
@@ -96,13 +100,46 @@ __global__ void __launch_bounds__(kLThreads) k_learned(LearnArgs LA) {
     }
     double m64 = kBig;
     d3 proj = {0.0, 0.0, 0.0};
-    const float r = valid ? A.radius[lin] : 0.f;
+    // no radius array: the same search with every bound infinite (it then starts from the seed)
+    const float r = !valid ? 0.f : (A.radius ? A.radius[lin] : INFINITY);
     // every triangle with FP64 distance <= r has FP32 distance <= lim_r
     const float lim_r = r + A.eD_abs + A.eD_rel * r;
     const float3 blo = make_float3(warp_min(valid ? p32.x : INFINITY), warp_min(valid ? p32.y : INFINITY),
                                    warp_min(valid ? p32.z : INFINITY));
     const float3 bhi = make_float3(warp_max(valid ? p32.x : -INFINITY), warp_max(valid ? p32.y : -INFINITY),
                                    warp_max(valid ? p32.z : -INFINITY));
+    // Seed: one greedy descent toward the brick's centre (the child whose box is nearer, all lanes
+    // reading the same node) to the first cluster, folded on every lane, so each lane has a
+    // minimum -- close to its own -- before the wide expansion begins.
+    {
+      const float3 bc = make_float3(0.5f * (blo.x + bhi.x), 0.5f * (blo.y + bhi.y), 0.5f * (blo.z + bhi.z));
+      int nid = 0, sfirst = 0, scnt = 0;
+      for (int depth = 0; depth < 128; ++depth) {
+        const BNode nd = A.nodes[nid];
+        float3 lo0, hi0, lo1, hi1;
+        child_box(nd, 0, lo0, hi0);
+        child_box(nd, 1, lo1, hi1);
+        const int gamma = nd.d.x & 0x7fffffff;
+        const int n0 = gamma - nd.d.z + 1, n1 = nd.d.w - gamma;
+        const float k0 = (lo0.x > hi0.x || n0 < 1) ? INFINITY : box_d2(bc, lo0, hi0);
+        const float k1 = (lo1.x > hi1.x || n1 < 1) ? INFINITY : box_d2(bc, lo1, hi1);
+        const bool right = k1 < k0;
+        const int cid = right ? nd.d.y : nd.d.x, cn = right ? n1 : n0;
+        if ((cid & kLeafBit) || cn <= kCluster) {
+          sfirst = right ? gamma + 1 : nd.d.z;
+          scnt = cn;
+          break;
+        }
+        nid = cid;
+      }
+      if (valid)
+        for (int t = 0; t < scnt; ++t) {
+          const int leaf = sfirst + t;
+          const float D = sqrtf(pt_tri_d2(p32, f3(LA.lv32[3 * leaf]), f3(LA.lv32[3 * leaf + 1]),
+                                          f3(LA.lv32[3 * leaf + 2])));
+          if (D <= lane_bound(A, L, lim_r, true)) lane_offer<kLThreads>(A, L, D, __float_as_int(LA.lbox[2 * leaf].w));
+        }
+    }
     bool ok = true, overflowed = false;
     int sp = 1, q = 0;
     if (lane == 0) stack[0] = 0;
@@ -122,6 +159,7 @@ __global__ void __launch_bounds__(kLThreads) k_learned(LearnArgs LA) {
         visits += n;
         bool push[2] = {false, false}, clu[2] = {false, false};
         int cid[2] = {0, 0}, first[2] = {0, 0}, cnt[2] = {0, 0};
+        float key[2] = {0.f, 0.f};
         float3 clo[2], chi[2];
         if (nid >= 0) {
           const BNode nd = A.nodes[nid];
@@ -137,10 +175,18 @@ __global__ void __launch_bounds__(kLThreads) k_learned(LearnArgs LA) {
 #pragma unroll
           for (int c = 0; c < 2; ++c) {
             if (clo[c].x > chi[c].x || cnt[c] < 1) continue;  // empty child
-            if (boxbox_d2(clo[c], chi[c], blo, bhi) > R2) continue;
+            key[c] = boxbox_d2(clo[c], chi[c], blo, bhi);
+            if (key[c] > R2) continue;
             if ((cid[c] & kLeafBit) || cnt[c] <= kCluster) clu[c] = true;
             else push[c] = true;
           }
+        }
+        // each lane's nearer child goes to the upper block (popped first)
+        const bool swap = push[0] && push[1] && key[1] < key[0];
+        if (swap) {
+          const int t = cid[0];
+          cid[0] = cid[1];
+          cid[1] = t;
         }
         const unsigned mp0 = __ballot_sync(0xffffffffu, push[0]), mp1 = __ballot_sync(0xffffffffu, push[1]);
         const unsigned mc0 = __ballot_sync(0xffffffffu, clu[0]), mc1 = __ballot_sync(0xffffffffu, clu[1]);
@@ -150,7 +196,7 @@ __global__ void __launch_bounds__(kLThreads) k_learned(LearnArgs LA) {
           overflowed = true;
           break;
         }
-        if (push[1]) stack[sp + __popc(mp1 & lt)] = cid[1];  // far-side children below, near-side on top
+        if (push[1]) stack[sp + __popc(mp1 & lt)] = cid[1];  // slot 1 below, slot 0 (the nearer) above
         if (push[0]) stack[sp + __popc(mp1) + __popc(mp0 & lt)] = cid[0];
         if (clu[0]) {
           const int at = q + __popc(mc0 & lt);
@@ -236,10 +282,136 @@ __global__ void __launch_bounds__(kLThreads) k_learned(LearnArgs LA) {
   }
 }
 
+// Exact unbounded distances of a sparse node set (the coarse grid the radius network trains on):
+// one thread per node walks the LBVH by itself, nearest child first, with a small stack of (node,
+// squared box distance) pairs, entering a child only when its box lies within band(m) of the node
+// (m: the FP32 minimum so far) and dropping stacked nodes that have fallen out of the bound without
+// loading them.  On a coarse grid neighbouring nodes are far apart, so a warp's walks share little
+// and a brick search would take the union of very different regions; per-thread walks do not.
+// Results are those of the other unbounded searches (FP64 resolution of the FP32 band in
+// ascending triangle index; FP64 re-search of a node whose band overflowed).
+constexpr int kPThreads = 128;
+constexpr int kTStack = 64;  // per-thread traversal stack (LBVH depth <= 64 for unique 64-bit keys)
+
+template <bool kExact>
+__device__ bool point_search(const LearnArgs& LA, const d3& p, const float3& p32, float lim_r, LaneBest& L,
+                             double& m64, d3& proj, int64_t& fp64, int64_t& visits) {
+  const UnbArgs& A = LA.u;
+  int st_id[kTStack];
+  float st_d[kTStack];
+  int sp = 0, cur = 0;
+  int64_t n = 0;
+  auto bound = [&]() -> float {
+    if (kExact) {
+      const float mf = (float)m64;
+      return fminf(lim_r, mf + A.eD_abs + A.eD_rel * mf);
+    }
+    return L.m < INFINITY ? fminf(lim_r, band_of(A, L.m)) : lim_r;
+  };
+  while (true) {
+    if (++n > A.max_visits) return false;
+    const BNode nd = A.nodes[cur];
+    float3 lo0, hi0, lo1, hi1;
+    child_box(nd, 0, lo0, hi0);
+    child_box(nd, 1, lo1, hi1);
+    const int c0 = nd.d.x, c1 = nd.d.y;
+    const float d0 = lo0.x > hi0.x ? INFINITY : box_d2(p32, lo0, hi0);
+    const float d1 = lo1.x > hi1.x ? INFINITY : box_d2(p32, lo1, hi1);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {  // leaf children, nearer first
+      const bool second = (k == 1) == (d0 <= d1);
+      const int c = second ? c1 : c0;
+      const float dc = second ? d1 : d0;
+      if (!(c & kLeafBit)) continue;
+      const float b = bound() + A.pad;
+      if (!(dc <= b * b)) continue;
+      const int leaf = c & 0x7fffffff;
+      const int prim = __float_as_int(LA.lbox[2 * leaf].w);
+      const float D = sqrtf(pt_tri_d2(p32, f3(LA.lv32[3 * leaf]), f3(LA.lv32[3 * leaf + 1]), f3(LA.lv32[3 * leaf + 2])));
+      if (D > bound()) continue;
+      if (kExact) {
+        step64_call(A.rec, prim, p, m64, proj);
+        ++fp64;
+      } else {
+        lane_offer<kPThreads>(A, L, D, prim);
+      }
+    }
+    const float b = bound() + A.pad, b2 = b * b;  // inner children: enter the nearer, stack the farther
+    const bool g0 = !(c0 & kLeafBit) && d0 <= b2, g1 = !(c1 & kLeafBit) && d1 <= b2;
+    if (g0 && g1) {
+      if (sp >= kTStack) return false;
+      const bool near0 = d0 <= d1;
+      st_id[sp] = near0 ? c1 : c0;
+      st_d[sp] = near0 ? d1 : d0;
+      ++sp;
+      cur = near0 ? c0 : c1;
+      continue;
+    }
+    if (g0 || g1) {
+      cur = g0 ? c0 : c1;
+      continue;
+    }
+    bool found = false;
+    while (sp > 0) {
+      --sp;
+      const float bb = bound() + A.pad;
+      if (st_d[sp] <= bb * bb) {
+        cur = st_id[sp];
+        found = true;
+        break;
+      }
+    }
+    if (!found) break;
+  }
+  visits += n;
+  return true;
+}
+
+__global__ void __launch_bounds__(kPThreads) k_nearest_points(LearnArgs LA) {
+  __shared__ int s_keep_t[kKeep * kPThreads];
+  __shared__ float s_keep_d[kKeep * kPThreads];
+  const UnbArgs& A = LA.u;
+  const GridP& g = A.g;
+  int64_t fp64 = 0, errs = 0, visits = 0;
+  for (int64_t lin = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; lin < g.ngp; lin += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = lin % g.n[0], j = (lin / g.n[0]) % g.n[1], k = lin / (g.n[0] * g.n[1]);
+    const d3 p = gnode(g, i, j, k);
+    const float3 p32 = local32(g, p);
+    LaneBest L;
+    L.m = INFINITY;
+    L.overflow = false;
+    L.t = s_keep_t + threadIdx.x;
+    L.d = s_keep_d + threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < kKeep; ++q) {
+      L.t[q * kPThreads] = -1;
+      L.d[q * kPThreads] = INFINITY;
+    }
+    double m64 = kBig;
+    d3 proj = {0.0, 0.0, 0.0};
+    bool ok = point_search<false>(LA, p, p32, INFINITY, L, m64, proj, fp64, visits);
+    if (ok && L.overflow) ok = point_search<true>(LA, p, p32, band_of(A, L.m), L, m64, proj, fp64, visits);
+    else if (ok) lane_resolve<kPThreads>(A, L, p, m64, proj, fp64);
+    if (!ok) ++errs;
+    A.dist[lin] = m64;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    fp64 += __shfl_down_sync(0xffffffffu, fp64, off);
+    errs += __shfl_down_sync(0xffffffffu, errs, off);
+    visits += __shfl_down_sync(0xffffffffu, visits, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (fp64) count_add(A.counters, C_FP64, fp64);
+    if (errs) count_add(A.counters, C_ERR_STACK, errs);
+    if (visits) count_add(A.counters, C_VISITS, visits);
+  }
+}
+
 }  // namespace
 
-// The learned-radius search over the grid g (radius: one FP32 bound per node, already computed).
-int run_learned(sdfgpu_ctx* ctx, const GridP& g, const float* radius, double* d_dist, double* d_xp) {
+namespace {
+
+LearnArgs learn_args(sdfgpu_ctx* ctx, const GridP& g, const float* radius, double* d_dist, double* d_xp) {
   const MeshDev& M = ctx->mesh;
   const float E = (float)g.E;
   LearnArgs LA;
@@ -265,8 +437,31 @@ int run_learned(sdfgpu_ctx* ctx, const GridP& g, const float* radius, double* d_
   }
   LA.lv32 = buf<float4>(ctx, "lv32");
   LA.lbox = buf<float4>(ctx, "lbox32");
+  A.next = nullptr;
   LA.max_rounds = 4 * M.nel + 64;  // every round expands at least one node or folds one cluster
-  k_learned<<<grid_for(A.nbricks, kLWarps, 148 * 16), kLThreads, 0, ctx->stream>>>(LA);
+  return LA;
+}
+
+}  // namespace
+
+// The learned-radius search over the grid g (radius: one FP32 bound per node, or NULL: unbounded).
+int run_learned(sdfgpu_ctx* ctx, const GridP& g, const float* radius, double* d_dist, double* d_xp) {
+  LearnArgs LA = learn_args(ctx, g, radius, d_dist, d_xp);
+  // one resident wave of CTAs draining the brick queue
+  SDF_TRY(scratch_t(ctx, "brick_next", 1, &LA.u.next));
+  SDF_CUDA(ctx, cudaMemsetAsync(LA.u.next, 0, sizeof(unsigned long long), ctx->stream));
+  int per_sm = 0, sms = 148;
+  SDF_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_learned, kLThreads, 0));
+  SDF_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  k_learned<<<grid_for(LA.u.nbricks, kLWarps, (int64_t)sms * (per_sm > 0 ? per_sm : 1)), kLThreads, 0, ctx->stream>>>(LA);
+  SDF_KERNEL(ctx);
+  return 0;
+}
+
+// Exact unbounded distances of the nodes of a sparse grid, one thread per node (no closest points).
+int run_nearest_points(sdfgpu_ctx* ctx, const GridP& g, double* d_dist) {
+  const LearnArgs LA = learn_args(ctx, g, nullptr, d_dist, nullptr);
+  k_nearest_points<<<grid_for(g.ngp, kPThreads, 148 * 16), kPThreads, 0, ctx->stream>>>(LA);
   SDF_KERNEL(ctx);
   return 0;
 }

@@ -584,16 +584,18 @@ int mlp_eval_host(sdfgpu_ctx* ctx, const float* params, const float* xn, const f
 int train_radius(sdfgpu_ctx* ctx, int coarse_n, int steps, int batch, float lr, uint64_t seed, float* final_loss) {
   cudaStream_t st = ctx->stream;
   const MeshDev& M = ctx->mesh;
-  // coarse grid: Grid(Xmin, Xmax, coarse_n - 7, 3), the rule of the workloads' grids
+  // coarse grid: coarse_n - 1 cells on the longest axis of the mesh box, padded by one cell (the
+  // workloads' grids pad by 3 of their own, much finer, cells); nodes far outside the box would only
+  // make the training targets expensive
   double o[3], amax[3], h;
   int64_t N[3], ngp;
   {
     const double ext = std::max(M.bmax[0] - M.bmin[0], std::max(M.bmax[1] - M.bmin[1], M.bmax[2] - M.bmin[2]));
-    h = ext / (double)(coarse_n - 7);
+    h = ext / (double)(coarse_n - 3);
     ngp = 1;
     for (int a = 0; a < 3; ++a) {
-      o[a] = M.bmin[a] - 3.0 * h;
-      N[a] = (int64_t)std::ceil((M.bmax[a] + 3.0 * h - o[a]) / h);
+      o[a] = M.bmin[a] - h;
+      N[a] = (int64_t)std::ceil((M.bmax[a] + h - o[a]) / h);
       amax[a] = o[a] + (double)N[a] * h;
       ngp *= N[a] + 1;
     }
@@ -602,7 +604,9 @@ int train_radius(sdfgpu_ctx* ctx, int coarse_n, int steps, int batch, float lr, 
   SDF_TRY(make_grid(ctx, o, h, N, g));
   double* dd;
   SDF_TRY(scratch_t(ctx, "mlp_dist", (size_t)ngp, &dd));
-  SDF_TRY(run_distances(ctx, g, SDFGPU_MODE_UNBOUNDED, 0, dd, nullptr));
+  // the exact unbounded distances of the coarse grid (sparse nodes: one nearest-first walk per node)
+  SDF_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_bvh, 0));
+  SDF_TRY(run_nearest_points(ctx, g, dd));
   RadiusNorm& R = ctx->radius;
   R.c[0] = 0.5 * (o[0] + amax[0]);
   R.c[1] = 0.5 * (o[1] + amax[1]);

@@ -27,11 +27,11 @@ struct RadiusNorm {
   double coarse_h = 0.0;
   float loss = 0.f;
   bool trained = false;
-  float alpha = 0.2f;  // radius margin: r = (dhat (1 + alpha) + beta coarse_h / s) s; the
-  float beta = 2.0f;   // fastest of the margins measured (it certifies every node on the workloads)
+  float alpha = 0.5f;  // radius margin: r = (dhat (1 + alpha) + beta coarse_h / s) s; the fastest
+  float beta = 4.0f;   // measured (tighter margins leave nodes uncertified, and those search twice)
   // options of the last training (what a SDFGPU_MODE_LEARNED batch trains every mesh with)
-  int train_coarse = 64, train_steps = 400, train_batch = 4096;
-  float train_lr = 3e-3f;
+  int train_coarse = 32, train_steps = 200, train_batch = 2048;
+  float train_lr = 5e-3f;
   uint64_t train_seed = 0;
 };
 

@@ -50,7 +50,16 @@ struct UnbArgs {
   int32_t b[3];         // brick of one warp: nodes along x, y, z (product 32)
   int64_t nb[3];        // bricks per axis
   int64_t nbricks;
+  unsigned long long* next;  // brick queue: warps take the next brick with one atomic (zeroed per launch)
 };
+
+// The warp's next brick from the launch's queue (bricks differ widely in cost, so a static split
+// leaves warps idle at the end); every lane gets the same index.
+__device__ __forceinline__ int64_t next_brick(const UnbArgs& A, int lane) {
+  unsigned long long b = 0ULL;
+  if (lane == 0) b = atomicAdd(A.next, 1ULL);
+  return (int64_t)__shfl_sync(0xffffffffu, b, 0);
+}
 
 // The FP64 step out of line: it is rare on this path, and inlining it would size the registers of
 // the whole traversal loop for it.

@@ -343,8 +343,9 @@ class Context:
         self._check(lib().sdfgpu_set_brick(self._p, b))
 
     # ---- learned search radius ----
-    def set_radius_margin(self, alpha=0.2, beta=2.0):
-        """r = (dhat (1 + alpha) + beta * coarse spacing / s) * s."""
+    def set_radius_margin(self, alpha=0.5, beta=4.0):
+        """r = (dhat (1 + alpha) + beta * coarse spacing / s) * s; alpha = inf: every radius infinite
+        (the learned mode's search without the network's bound)."""
         self._check(lib().sdfgpu_set_radius_margin(self._p, float(alpha), float(beta)))
 
     def train_radius(self, coarse_n=64, steps=1500, batch=8192, lr=2e-3, seed=0):
