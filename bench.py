@@ -516,6 +516,9 @@ def main():
     ap.add_argument("--variant-steps", type=int, default=3, help="timed steps of the plain and ref-rule SDF forms")
     ap.add_argument("--ref-sample", type=int, default=1 << 14)
     ap.add_argument("--streams", type=int, default=8, help="batch workloads: worker streams")
+    ap.add_argument("--once", action="store_true",
+                    help="run one untimed learned-form step (set_mesh, train_radius, sdf) and exit: the "
+                         "kernel sequence a profiler captures")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.steps is None:
@@ -543,6 +546,15 @@ def main():
 
     if args.workload.startswith("batch"):
         return run_batch(args, rank, world, local)
+    if args.once:
+        X, IEN, g = load_gpu(args.workload, local)
+        ctx = _native.Context(local)
+        ctx.set_mesh(X, IEN)
+        ctx.train_radius(**TRAIN)
+        ctx.sdf(g["origin"], g["h"], g["N"], mode=_native.MODE_LEARNED)
+        print(json.dumps({"once": args.workload, "ms_distance": ctx.stats()["ms_distance"]}), flush=True)
+        ctx.close()
+        return 0
     if args.split == "zslab" and dist_on:
         return run_zslab(args, rank, world, local)
     X, IEN, g = load_gpu(args.workload, local)
