@@ -43,15 +43,6 @@ struct LearnArgs {
   int64_t max_rounds;  // bound on the expansion rounds of one brick
 };
 
-// Per-warp state of the packed cluster fold: each lane's first pair, cluster mask, node and bound,
-// and one result byte per (lane, cluster) pair of the batch (at most 32 x 32).
-struct PackState {
-  int off[32];
-  unsigned mask[32];
-  float4 pt[32];
-  uint8_t res[32 * 32];
-};
-
 // Squared distance between two boxes.
 __device__ __forceinline__ float boxbox_d2(float3 alo, float3 ahi, float3 blo, float3 bhi) {
   const float dx = fmaxf(fmaxf(alo.x - bhi.x, blo.x - ahi.x), 0.f);
@@ -81,12 +72,10 @@ __global__ void __launch_bounds__(kLThreads) k_learned(LearnArgs LA) {
   __shared__ float4 s_q[kLWarps][kLQueue][2];
   __shared__ int s_keep_t[kKeep * kLThreads];
   __shared__ float s_keep_d[kKeep * kLThreads];
-  __shared__ PackState s_pk[kLWarps];
   const UnbArgs& A = LA.u;
   const GridP& g = A.g;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int* stack = s_stack[w];
-  PackState& PK = s_pk[w];
   float4(*Q)[2] = s_q[w];
   const unsigned lt = (1u << lane) - 1u;  // lanes below this one
   const int lx = lane % A.b[0], ly = (lane / A.b[0]) % A.b[1], lz = lane / (A.b[0] * A.b[1]);
@@ -227,74 +216,27 @@ __global__ void __launch_bounds__(kLThreads) k_learned(LearnArgs LA) {
       // most 64) clusters fit the queue
       while (q >= 32 || (sp == 0 && q > 0)) {
         const int kq = min(q, 32), base = q - kq;
-        const float lim = lane_bound(A, L, lim_r, valid);
-        const float lb = lim + A.pad;
+        float lim = lane_bound(A, L, lim_r, valid);
+        float lb = lim + A.pad;
         unsigned mask = 0u;
         for (int c = 0; c < kq; ++c) {
           const float4 a = Q[base + c][0], b = Q[base + c][1];
           if (box_d2(p32, make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z)) <= lb * lb) mask |= 1u << c;
         }
         if (!valid) mask = 0u;
-        // The (lane, cluster) pairs of the batch, lane-major: lane j owns pairs off[j] .. off[j+1]-1.
-        const int own = __popc(mask);
-        int incl = own;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-          const int v = __shfl_up_sync(0xffffffffu, incl, d);
-          if (lane >= d) incl += v;
-        }
-        const int excl = incl - own;
-        const int P = __shfl_sync(0xffffffffu, incl, 31);
-        PK.off[lane] = excl;
-        PK.mask[lane] = mask;
-        PK.pt[lane] = make_float4(p32.x, p32.y, p32.z, lim);
-        __syncwarp();
-        // Packed filter: lane k takes pair k (owner j, cluster c) and tests c's triangles against j's
-        // bound at the start of the batch, all lanes busy; bit t of res[k] marks triangle t within it.
-        for (int k0 = 0; k0 < P; k0 += 32) {
-          const int k = k0 + lane;
-          if (k < P) {
-            int lo = 0, hi = 31;  // owner: the last lane whose first pair is <= k (it owns at least one)
-            while (lo < hi) {
-              const int mid = (lo + hi + 1) >> 1;
-              if (PK.off[mid] <= k) lo = mid;
-              else hi = mid - 1;
-            }
-            unsigned mj = PK.mask[lo];
-            for (int u = k - PK.off[lo]; u > 0; --u) mj &= mj - 1u;
-            const int c = __ffs(mj) - 1;
-            const float4 pt = PK.pt[lo];
-            const float3 pj = make_float3(pt.x, pt.y, pt.z);
-            const float lbj = pt.w + A.pad;
-            const int f0 = __float_as_int(Q[base + c][0].w), nleaf = __float_as_int(Q[base + c][1].w);
-            unsigned bits = 0u;
-            for (int t = 0; t < nleaf; ++t) {
-              const int leaf = f0 + t;
-              const float4 bl = LA.lbox[2 * leaf], bh = LA.lbox[2 * leaf + 1];
-              if (box_d2(pj, make_float3(bl.x, bl.y, bl.z), make_float3(bh.x, bh.y, bh.z)) > lbj * lbj) continue;
-              const float D = sqrtf(pt_tri_d2(pj, f3(LA.lv32[3 * leaf]), f3(LA.lv32[3 * leaf + 1]),
-                                              f3(LA.lv32[3 * leaf + 2])));
-              if (D <= pt.w) bits |= 1u << t;
-            }
-            PK.res[k] = (uint8_t)bits;
-          }
-        }
-        __syncwarp();
-        // Each lane offers its own marked triangles (the same FP32 distances), in cluster order.
-        unsigned mm = mask;
-        for (int k = excl; k < excl + own; ++k) {
-          const int c = __ffs(mm) - 1;
-          mm &= mm - 1u;
-          unsigned bits = PK.res[k];
-          if (!bits) continue;
-          const int f0 = __float_as_int(Q[base + c][0].w);
-          while (bits) {
-            const int t = __ffs(bits) - 1;
-            bits &= bits - 1u;
+        while (mask) {
+          const int c = __ffs(mask) - 1;
+          mask &= mask - 1u;
+          const int f0 = __float_as_int(Q[base + c][0].w), nleaf = __float_as_int(Q[base + c][1].w);
+          for (int t = 0; t < nleaf; ++t) {
             const int leaf = f0 + t;
+            const float4 bl = LA.lbox[2 * leaf], bh = LA.lbox[2 * leaf + 1];
+            lim = lane_bound(A, L, lim_r, true);
+            lb = lim + A.pad;
+            if (box_d2(p32, make_float3(bl.x, bl.y, bl.z), make_float3(bh.x, bh.y, bh.z)) > lb * lb) continue;
             const float D = sqrtf(pt_tri_d2(p32, f3(LA.lv32[3 * leaf]), f3(LA.lv32[3 * leaf + 1]),
                                             f3(LA.lv32[3 * leaf + 2])));
-            if (D <= lane_bound(A, L, lim_r, true)) lane_offer<kLThreads>(A, L, D, __float_as_int(LA.lbox[2 * leaf].w));
+            if (D <= lim) lane_offer<kLThreads>(A, L, D, __float_as_int(bl.w));
           }
         }
         q = base;
