@@ -614,9 +614,10 @@ def main():
             forms[name] = f
         forms["learned_vs_plain_unbounded_sdf"] = value / forms["plain_unbounded"]["value"]
 
-    # HBM roofline of the dominant kernel (the learned search): algorithmic bytes per launch = the
-    # radius read and the distance written per node (4 + 8 B) + the triangle data read once (FP32
-    # vertices 48 B, FP64 record 352 B) + the LBVH nodes read once (64 B per inner node).
+    # HBM roofline of the dominant kernel (k_unbounded, the packet search bounded by the learned
+    # radius): algorithmic bytes per launch = the radius read and the distance written per node
+    # (4 + 8 B) + the triangle data read once (FP32 vertices 48 B, FP64 record 352 B) + the LBVH read
+    # once (64 B node and 128 B of oriented child boxes per inner node).
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
         peaks = json.load(open(peaks_path))
@@ -624,12 +625,12 @@ def main():
     else:
         peak, peak_src = 6650.0, "fallback"
     search_ms = sum(learned.fold_ms) / len(learned.fold_ms)
-    alg_bytes = 12 * ngp + 400 * IEN.shape[0] + 64 * (IEN.shape[0] - 1)
+    alg_bytes = 12 * ngp + 400 * IEN.shape[0] + 192 * (IEN.shape[0] - 1)
     achieved = alg_bytes / (search_ms / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(args.workload, {}).get("k_learned")
+        traffic = json.load(open(tpath)).get(args.workload, {}).get("k_unbounded")
 
     # FP32 roofline of the same kernel (the path's real bound: CUDA-core arithmetic): the oracle's
     # work model gives the algorithmic FP32 FLOPs per node of the unbounded nearest search, F_pt |D*_u|
@@ -644,7 +645,7 @@ def main():
         w = wm["mean_W_dist_unbounded_flop"]
         bound = p32 * 1e12 / w
         ach = ngp / (search_ms / 1e3)
-        roof32 = {"bound": "fp32", "kernel": "k_learned", "mean_W_flop_per_node": w, "F_pt": wm["F_pt"],
+        roof32 = {"bound": "fp32", "kernel": "k_unbounded", "mean_W_flop_per_node": w, "F_pt": wm["F_pt"],
                   "work_sample": wm["sample"], "peak": p32, "unit": "TFLOP/s", "peak_source": "measured (FMA probe)",
                   "achieved": ach * w / 1e12, "roofline_nodes_per_s": bound, "frac": ach / bound,
                   "step_frac": value / world / (p32 * 1e12 / wm["mean_W_flop"]) if wm.get("mean_W_flop") else None}
@@ -660,7 +661,7 @@ def main():
         "e2e": {"value": e2e_value, "unit": "nodes/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps},
         "gpu_launches": int(learned.launches),
-        "roofline": {"bound": "hbm", "kernel": "k_learned", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": "k_unbounded", "achieved": achieved, "peak": peak,
                      "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "alg_bytes_per_launch": int(alg_bytes), "ms_per_launch": search_ms},
         "roofline_fp32": roof32,

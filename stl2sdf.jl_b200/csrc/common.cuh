@@ -25,6 +25,9 @@ struct __align__(16) BNode {
   int4 d;    // left, right, parent, unused
 };
 constexpr int32_t kLeafBit = (int32_t)0x80000000;
+// Child subtrees of 2..kObbMaxLeaves leaves carry an oriented box (OBox, "obb" buffer) besides
+// their axis-aligned one; above this size a patch is no longer flat and the box would not pay.
+constexpr int kObbMaxLeaves = 4096;
 
 // Device counters (int64) zeroed at the start of every grid call.
 enum Counter : int {
@@ -222,8 +225,6 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
                           bool device_ptrs);
 int ensure_ine(sdfgpu_ctx* ctx);
 int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, double* d_dist, double* d_xp);
-// The learned-radius nearest-triangle search (learned.cu) with one FP32 radius per node.
-int run_learned(sdfgpu_ctx* ctx, const GridP& g, const float* radius, double* d_dist, double* d_xp);
 // Exact unbounded distances of a sparse grid's nodes, one thread per node (learned.cu).
 int run_nearest_points(sdfgpu_ctx* ctx, const GridP& g, double* d_dist);
 

@@ -603,12 +603,10 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
         SDF_TRY(scratch_t(ctx, "radius", (size_t)g.ngp, &radius));
         SDF_TRY(run_radius(ctx, &g, nullptr, g.ngp, R.alpha, (float)(R.beta * R.coarse_h / R.s), radius));
       }
-      SDF_MARK(ctx, T_TILES);
-      SDF_TRY(run_learned(ctx, g, radius, d_dist, d_xp));
-      SDF_MARK(ctx, T_FOLD);
-      return 0;
     }
-    UnbArgs A{g, nodes, leaf_prim, v32, rec, pad, eD_abs, eD_rel, 2 * nel + 64, radius, d_dist, d_xp, ctx->d_counters};
+    UnbArgs A{g, nodes, leaf_prim, v32, rec, kUnbPadRel * E, eD_abs, eD_rel, 2 * nel + 64, radius, d_dist, d_xp,
+              ctx->d_counters};
+    A.obb = buf<OBox>(ctx, "obb");
     A.nbricks = 1;
     for (int a = 0; a < 3; ++a) {
       A.b[a] = ctx->brick[a];

@@ -47,6 +47,28 @@ __device__ __forceinline__ float pt_tri_d2(float3 p, float3 a, float3 b, float3 
   return d2;
 }
 
+// Oriented box of an LBVH child subtree (mesh-local FP32).  For every vertex x of the subtree's
+// triangles, and so for every point of them, |x . a_k - c_k| <= e_k along the three stored axes
+// a_k (the inequality holds in exact arithmetic on the stored FP32 values).  a0..a2 hold
+// (a_k.x, a_k.y, a_k.z, c_k), e holds (e_0, e_1, e_2, 0).  A child without a fitted box carries
+// extents kNoObb, for which the bound below is 0.
+struct __align__(16) OBox {
+  float4 a0, a1, a2, e;
+};
+constexpr float kNoObb = 3.0e38f;
+
+// Squared lower bound on the distance from p to the points of an oriented box: the axes are
+// orthonormal to FP32 rounding, so the sum over axes of (|p . a_k - c_k| - e_k)_+^2 is the squared
+// distance to the box up to a relative 1e-6 (callers add an absolute margin for it and for the
+// rounding of this evaluation).
+__device__ __forceinline__ float obox_d2(float3 p, const OBox& o) {
+  const float t0 = fabsf(fmaf(p.x, o.a0.x, fmaf(p.y, o.a0.y, fmaf(p.z, o.a0.z, -o.a0.w)))) - o.e.x;
+  const float t1 = fabsf(fmaf(p.x, o.a1.x, fmaf(p.y, o.a1.y, fmaf(p.z, o.a1.z, -o.a1.w)))) - o.e.y;
+  const float t2 = fabsf(fmaf(p.x, o.a2.x, fmaf(p.y, o.a2.y, fmaf(p.z, o.a2.z, -o.a2.w)))) - o.e.z;
+  const float u0 = fmaxf(t0, 0.f), u1 = fmaxf(t1, 0.f), u2 = fmaxf(t2, 0.f);
+  return fmaf(u0, u0, fmaf(u1, u1, u2 * u2));
+}
+
 // Squared distance from p to the box [lo, hi].
 __device__ __forceinline__ float box_d2(float3 p, float3 lo, float3 hi) {
   const float dx = fmaxf(fmaxf(lo.x - p.x, p.x - hi.x), 0.f);

@@ -1,12 +1,15 @@
-// unbounded.cuh -- the nearest-triangle search of SDFGPU_MODE_UNBOUNDED shared by the plain
-// packet traversal (k_unbounded, distance.cu) and the learned-radius search (k_learned,
-// learned.cu): the kernel arguments, the per-lane FP32 band of candidate triangles with its FP64
-// resolution in ascending triangle index, and the warp's packet traversal of the LBVH.
+// unbounded.cuh -- the nearest-triangle search of SDFGPU_MODE_UNBOUNDED and SDFGPU_MODE_LEARNED:
+// the kernel arguments, the per-lane FP32 band of candidate triangles with its FP64 resolution in
+// ascending triangle index, and the warp's packet traversal of the LBVH (k_unbounded,
+// distance.cu; the per-node walk of the training grid, learned.cu, shares the band).
 //
-// Both kernels return, for every node, the FP64 minimum over all triangles of the point-triangle
+// Every search returns, for each node, the FP64 minimum over all triangles of the point-triangle
 // distance (tri_step64 without the vertex-skip rule), ties to the lowest triangle index -- the
 // result of folding every triangle in index order (dfOnTriangularMesh.jl:101-177 with the true
-// minimum).  The FP32 search only decides which triangles can hold that minimum.
+// minimum).  The FP32 search only decides which triangles can hold that minimum: a child subtree
+// is entered when the larger of its axis-aligned and its oriented box distance (OBox, mesh.cu)
+// lies within the lane's bound plus the FP32 margin kUnbPadRel E.
+
 #pragma once
 
 #include "common.cuh"
@@ -51,7 +54,30 @@ struct UnbArgs {
   int64_t nb[3];        // bricks per axis
   int64_t nbricks;
   unsigned long long* next;  // brick queue: warps take the next brick with one atomic (zeroed per launch)
+  const OBox* obb;           // oriented boxes of the LBVH children (obb[2 node + side])
 };
+
+// FP32 margin of every box test of the unbounded searches, as a multiple of the frame's scale E:
+// 2e-6 E for the FP32 point-triangle distance and the axis-aligned box distance, plus 2e-5 E for
+// the oriented-box bound (its FP32 evaluation and the FP32 rounding of its axes stay below
+// 2.3e-6 E for points within E of the centre on every axis).
+constexpr float kUnbPadRel = 2.2e-5f;
+
+// Squared lower bound on the distance from p to the child `side` of LBVH node nid: the larger of
+// its axis-aligned and its oriented box (leaves: the axis-aligned box only).
+__device__ __forceinline__ float child_d2(const UnbArgs& A, const BNode& nd, int nid, int side, float3 p, float3 lo,
+                                          float3 hi) {
+  const float d = box_d2(p, lo, hi);
+  const int c = side ? nd.d.y : nd.d.x;
+  if (c & kLeafBit) return d;
+  return fmaxf(d, obox_d2(p, A.obb[2 * nid + side]));
+}
+__device__ __forceinline__ float child_d2(const BNode& nd, const OBox& o, int side, float3 p, float3 lo, float3 hi) {
+  const float d = box_d2(p, lo, hi);
+  const int c = side ? nd.d.y : nd.d.x;
+  if (c & kLeafBit) return d;
+  return fmaxf(d, obox_d2(p, o));
+}
 
 // The warp's next brick from the launch's queue (bricks differ widely in cost, so a static split
 // leaves warps idle at the end); every lane gets the same index.
@@ -132,12 +158,14 @@ __device__ bool warp_search(const UnbArgs& A, int* stack, int lane, int rep, con
     if (++visits > A.max_visits) { ok = false; break; }
     const int nid = stack[--sp];
     __syncwarp();
+    // the node and both oriented boxes in one round of loads (leaf children carry kNoObb boxes)
     const BNode nd = A.nodes[nid];
+    const OBox ob0 = A.obb[2 * nid], ob1 = A.obb[2 * nid + 1];
     float3 lo0, hi0, lo1, hi1;
     child_box(nd, 0, lo0, hi0);
     child_box(nd, 1, lo1, hi1);
     const bool e0 = lo0.x > hi0.x, e1 = lo1.x > hi1.x;  // empty child
-    const float d0 = box_d2(p32, lo0, hi0), d1 = box_d2(p32, lo1, hi1);
+    const float d0 = child_d2(nd, ob0, 0, p32, lo0, hi0), d1 = child_d2(nd, ob1, 1, p32, lo1, hi1);
     float lim;
     if (kExact) {
       const float mf = (float)m64;
