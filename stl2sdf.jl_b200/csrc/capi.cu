@@ -255,7 +255,7 @@ int run_all(sdfgpu_ctx* ctx, const GridP& g, bool want_dist, bool want_sign, int
   auto join = [&]() {
     if (forked && cudaEventRecord(ctx->ev_join, ss) == cudaSuccess) cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0);
     forked = false;
-    cudaStreamWaitEvent(ctx->stream, ctx->ev_bvh, 0);
+    cudaStreamWaitEvent(ctx->stream, ctx->ev_obb, 0);
   };
   auto stages = [&]() -> int {
     if (want_sign) {
@@ -404,7 +404,7 @@ int create_context(const sdfgpu_opts* opts, sdfgpu_ctx** out, bool stage_priorit
     return bail("cudaStreamCreate", e);
   if ((e = cudaStreamCreateWithPriority(&ctx->bvh_stream, cudaStreamNonBlocking, stage_prio)) != cudaSuccess)
     return bail("cudaStreamCreate", e);
-  for (cudaEvent_t* ev : {&ctx->ev_fork, &ctx->ev_join, &ctx->ev_rows, &ctx->ev_mesh, &ctx->ev_bvh})
+  for (cudaEvent_t* ev : {&ctx->ev_fork, &ctx->ev_join, &ctx->ev_rows, &ctx->ev_mesh, &ctx->ev_bvh, &ctx->ev_obb})
     if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return bail("cudaEventCreate", e);
   if ((e = cudaHostAlloc((void**)&ctx->h_scalars, sizeof(int64_t) * S_NUM, cudaHostAllocDefault)) != cudaSuccess)
     return bail("cudaHostAlloc", e);
@@ -453,7 +453,7 @@ int sdfgpu_destroy(sdfgpu_ctx* ctx) {
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : ctx->tev)
     if (ev) cudaEventDestroy(ev);
-  for (cudaEvent_t ev : {ctx->ev_fork, ctx->ev_join, ctx->ev_rows, ctx->ev_mesh, ctx->ev_bvh})
+  for (cudaEvent_t ev : {ctx->ev_fork, ctx->ev_join, ctx->ev_rows, ctx->ev_mesh, ctx->ev_bvh, ctx->ev_obb})
     if (ev) cudaEventDestroy(ev);
   if (ctx->bvh_stream) cudaStreamDestroy(ctx->bvh_stream);
   if (ctx->h_scalars) cudaFreeHost(ctx->h_scalars);

@@ -116,6 +116,7 @@ struct sdfgpu_ctx {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_rows = nullptr;
   cudaEvent_t ev_mesh = nullptr;         // triangle records ready (on the context stream)
   cudaEvent_t ev_bvh = nullptr;          // LBVH of the current mesh complete (on bvh_stream)
+  cudaEvent_t ev_obb = nullptr;          // its oriented child boxes complete too (on bvh_stream, after ev_bvh)
   int64_t* h_scalars = nullptr;          // page-locked host slots for sizing reads (see Scalar)
   std::string ns;                        // prefix of every scratch-buffer name (batch items keep their own)
   std::vector<sdfgpu_ctx*> workers;      // batch workers (batch.cu), created on first use

@@ -495,7 +495,7 @@ __global__ void k_knn_fallback(KnnArgs A) {
 // nearer triangle lies within r and was visited), and the lanes without one search again without
 // the bound, keeping what they found.  Lanes whose band overflowed search once more with FP64
 // steps bounded by the band.
-__global__ void __launch_bounds__(kUnbThreads, 3) k_unbounded(UnbArgs A) {
+__global__ void __launch_bounds__(kUnbThreads, 4) k_unbounded(UnbArgs A) {
   __shared__ int s_stack[kUnbWarps][kWarpStack];
   __shared__ int s_keep_t[kKeep * kUnbThreads];
   __shared__ float s_keep_d[kKeep * kUnbThreads];
@@ -592,7 +592,7 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
   const float pad = 2.0e-6f * E;
 
   if (mode == SDFGPU_MODE_UNBOUNDED) {
-    SDF_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_bvh, 0));  // the search walks the LBVH
+    SDF_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_obb, 0));  // the search walks the LBVH and its oriented boxes
     float* radius = nullptr;
     if (use_learned) {
       // r = (dhat (1 + alpha) + beta * coarse spacing / s) s: a margin for the network's error and

@@ -255,122 +255,187 @@ __global__ void k_leaf_order(const int32_t* __restrict__ leaf_prim, const float4
   }
 }
 
-__device__ __forceinline__ double warp_sum_d(double v) {
-  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-  return v;
-}
-
-// Eigenvectors of the symmetric 3x3 matrix A (cyclic Jacobi rotations, a fixed number of sweeps):
-// the columns of V, orthonormal to FP64 rounding whatever the input.
-__device__ void jacobi3(double A[3][3], double V[3][3]) {
+// Eigenvectors of the symmetric 3x3 matrix A (cyclic Jacobi rotations in FP32, at most 8 sweeps):
+// the columns of V, orthonormal to a few FP32 roundings.
+__device__ void jacobi3f(float A[3][3], float V[3][3]) {
   for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) V[i][j] = i == j ? 1.0 : 0.0;
-  for (int sweep = 0; sweep < 12; ++sweep) {
-    const double off = fabs(A[0][1]) + fabs(A[0][2]) + fabs(A[1][2]);
-    const double diag = fabs(A[0][0]) + fabs(A[1][1]) + fabs(A[2][2]);
-    if (!(off > 1e-18 * diag)) break;
-    for (int p = 0; p < 2; ++p)
-      for (int q = p + 1; q < 3; ++q) {
-        const double apq = A[p][q];
-        if (apq == 0.0) continue;
-        const double th = (A[q][q] - A[p][p]) / (2.0 * apq);
-        const double t = (th >= 0.0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
-        const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
-        for (int k = 0; k < 3; ++k) {
-          const double akp = A[k][p], akq = A[k][q];
-          A[k][p] = c * akp - s * akq;
-          A[k][q] = s * akp + c * akq;
-        }
-        for (int k = 0; k < 3; ++k) {
-          const double apk = A[p][k], aqk = A[q][k];
-          A[p][k] = c * apk - s * aqk;
-          A[q][k] = s * apk + c * aqk;
-        }
-        for (int k = 0; k < 3; ++k) {
-          const double vkp = V[k][p], vkq = V[k][q];
-          V[k][p] = c * vkp - s * vkq;
-          V[k][q] = s * vkp + c * vkq;
-        }
+    for (int j = 0; j < 3; ++j) V[i][j] = i == j ? 1.f : 0.f;
+#pragma unroll 1
+  for (int sweep = 0; sweep < 8; ++sweep) {
+    const float off = fabsf(A[0][1]) + fabsf(A[0][2]) + fabsf(A[1][2]);
+    const float diag = fabsf(A[0][0]) + fabsf(A[1][1]) + fabsf(A[2][2]);
+    if (!(off > 1e-7f * diag)) break;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const int p = r == 2 ? 1 : 0, q = r == 0 ? 1 : 2;
+      const float apq = A[p][q];
+      if (apq == 0.f) continue;
+      const float th = (A[q][q] - A[p][p]) / (2.f * apq);
+      const float t = copysignf(1.f, th) / (fabsf(th) + sqrtf(fmaf(th, th, 1.f)));
+      const float c = rsqrtf(fmaf(t, t, 1.f)), sn = t * c;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const float akp = A[k][p], akq = A[k][q];
+        A[k][p] = c * akp - sn * akq;
+        A[k][q] = sn * akp + c * akq;
       }
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const float apk = A[p][k], aqk = A[q][k];
+        A[p][k] = c * apk - sn * aqk;
+        A[q][k] = sn * apk + c * aqk;
+      }
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const float vkp = V[k][p], vkq = V[k][q];
+        V[k][p] = c * vkp - sn * vkq;
+        V[k][q] = sn * vkp + c * vkq;
+      }
+    }
   }
 }
 
-// Oriented boxes of the LBVH's children (OBox, two per inner node: obb[2 i + side]).  One warp per
-// inner node fits, for each child subtree of 2..kObbMaxLeaves leaves (a contiguous run of the
-// Morton-sorted leaves), the principal axes of its vertices -- the FP64 covariance about the run's
-// first vertex, diagonalised by Jacobi rotations -- and then the exact extents of its FP32 vertices
-// along the axes as stored in FP32.  The axes only decide how tight the box is; the extents make
-// it a bound for whatever axes come out.  On a smooth surface the smallest axis is the patch
-// normal and the box is a thin slab around the patch, so a point at distance D from the surface
-// has a lower bound close to D for every patch away from its nearest point (an axis-aligned box
-// of a tilted patch is as thick as the patch is wide).  Leaves and larger subtrees get kNoObb.
-__global__ void k_obb(const BNode* __restrict__ nodes, const float4* __restrict__ lv32, int n_inner, double E,
-                      OBox* __restrict__ obb) {
-  const int lane = threadIdx.x & 31;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n_inner; i += nw) {
-    const int4 d = nodes[i].d;
-    const int gamma = d.x & 0x7fffffff;  // the left child covers leaves [d.z, gamma], the right [gamma + 1, d.w]
-#pragma unroll 1
-    for (int side = 0; side < 2; ++side) {
-      const int first = side ? gamma + 1 : d.z;
-      const int cnt = side ? d.w - gamma : gamma - d.z + 1;
-      OBox o;
+template <bool kWarp>
+__device__ __forceinline__ double red_sum(double v) {
+  if (kWarp)
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+// The oriented box of the leaves [first, first + cnt) (see k_obb_small); kWarp: the 32 lanes of a
+// warp share the loops over the vertices and all return the same box.
+template <bool kWarp>
+__device__ OBox fit_obox(const float4* __restrict__ lv32, int first, int cnt, double E, int lane) {
+  const int step = kWarp ? 32 : 1, start = first + (kWarp ? lane : 0), end = first + cnt;
+  const float4 r4 = lv32[3 * first];
+  const double rx = r4.x, ry = r4.y, rz = r4.z;
+  double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // sums of x, y, z, xx, xy, xz, yy, yz, zz about the first vertex
+  for (int l = start; l < end; l += step)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float4 v = lv32[3 * l + k];
+      const double x = v.x - rx, y = v.y - ry, z = v.z - rz;
+      s[0] += x; s[1] += y; s[2] += z;
+      s[3] = fma(x, x, s[3]); s[4] = fma(x, y, s[4]); s[5] = fma(x, z, s[5]);
+      s[6] = fma(y, y, s[6]); s[7] = fma(y, z, s[7]); s[8] = fma(z, z, s[8]);
+    }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) s[k] = red_sum<kWarp>(s[k]);
+  const double nv = 3.0 * cnt, mx = s[0] / nv, my = s[1] / nv, mz = s[2] / nv;
+  const double c00 = s[3] / nv - mx * mx, c01 = s[4] / nv - mx * my, c02 = s[5] / nv - mx * mz;
+  const double c11 = s[6] / nv - my * my, c12 = s[7] / nv - my * mz, c22 = s[8] / nv - mz * mz;
+  const double tr = c00 + c11 + c22;
+  double ax[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  if (tr > 0.0) {  // principal axes of the trace-normalised covariance (FP32 is enough for a direction)
+    const double inv = 1.0 / tr;
+    float A[3][3] = {{(float)(c00 * inv), (float)(c01 * inv), (float)(c02 * inv)},
+                     {(float)(c01 * inv), (float)(c11 * inv), (float)(c12 * inv)},
+                     {(float)(c02 * inv), (float)(c12 * inv), (float)(c22 * inv)}};
+    float V[3][3];
+    jacobi3f(A, V);
+    // Gram-Schmidt in FP64: the axes are orthonormal to FP64 rounding before they are stored in FP32
+    double a[3] = {V[0][0], V[1][0], V[2][0]}, b[3] = {V[0][1], V[1][1], V[2][1]};
+    const double na = 1.0 / sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    for (int k = 0; k < 3; ++k) a[k] *= na;
+    const double ab = a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+    for (int k = 0; k < 3; ++k) b[k] -= ab * a[k];
+    const double bb = b[0] * b[0] + b[1] * b[1] + b[2] * b[2];
+    if (bb > 1e-12) {
+      const double nb = 1.0 / sqrt(bb);
+      for (int k = 0; k < 3; ++k) {
+        ax[0][k] = a[k];
+        ax[1][k] = b[k] * nb;
+      }
+      ax[2][0] = ax[0][1] * ax[1][2] - ax[0][2] * ax[1][1];
+      ax[2][1] = ax[0][2] * ax[1][0] - ax[0][0] * ax[1][2];
+      ax[2][2] = ax[0][0] * ax[1][1] - ax[0][1] * ax[1][0];
+    }
+  }
+  float af[3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int k = 0; k < 3; ++k) af[a][k] = (float)ax[a][k];
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int l = start; l < end; l += step)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float4 v = lv32[3 * l + k];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {  // float x float products are exact in FP64
+        const double t = (double)v.x * af[a][0] + (double)v.y * af[a][1] + (double)v.z * af[a][2];
+        lo[a] = fmin(lo[a], t);
+        hi[a] = fmax(hi[a], t);
+      }
+    }
+  OBox o;
+  float ce[3], ex[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (kWarp)
+      for (int off = 16; off > 0; off >>= 1) {
+        lo[a] = fmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], off));
+        hi[a] = fmax(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], off));
+      }
+    const double c = 0.5 * (lo[a] + hi[a]);
+    ce[a] = (float)c;
+    // the FP64 sums above round by at most ~1e-15 E; the margin 1e-9 E covers them
+    ex[a] = __double2float_ru(0.5 * (hi[a] - lo[a]) + fabs(c - (double)ce[a]) + 1e-9 * E);
+  }
+  o.a0 = make_float4(af[0][0], af[0][1], af[0][2], ce[0]);
+  o.a1 = make_float4(af[1][0], af[1][1], af[1][2], ce[1]);
+  o.a2 = make_float4(af[2][0], af[2][1], af[2][2], ce[2]);
+  o.e = make_float4(ex[0], ex[1], ex[2], 0.f);
+  return o;
+}
+
+// The child `side` of inner node i covers the sorted leaves [first, first + cnt): the left child
+// [d.z, gamma], the right [gamma + 1, d.w].
+__device__ __forceinline__ void child_range(const BNode* nodes, int i, int side, int& first, int& cnt) {
+  const int4 d = nodes[i].d;
+  const int gamma = d.x & 0x7fffffff;
+  first = side ? gamma + 1 : d.z;
+  cnt = side ? d.w - gamma : gamma - d.z + 1;
+}
+
+constexpr int kObbWarpMin = 33;  // children of this many leaves or more are fitted by a warp
+
+// Oriented boxes of the LBVH's children (OBox, two per inner node: obb[2 i + side]).  For each child
+// subtree of 2..kObbMaxLeaves leaves (a contiguous run of the Morton-sorted leaves) the principal
+// axes of its vertices -- the FP64 covariance about the run's first vertex, diagonalised by Jacobi
+// rotations -- and then the exact extents of its FP32 vertices along the axes as stored.  The axes
+// only decide how tight the box is; the extents make it a bound for whatever axes come out.  On a
+// smooth surface the smallest axis is the patch normal and the box is a thin slab around the patch,
+// so a point at distance D from the surface has a lower bound close to D for every patch away from
+// its nearest point (an axis-aligned box of a tilted patch is as thick as the patch is wide).
+// Leaves and larger subtrees get kNoObb.  One thread per child here; children of kObbWarpMin or
+// more leaves are left to k_obb_large (one warp per child).
+__global__ void k_obb_small(const BNode* __restrict__ nodes, const float4* __restrict__ lv32, int n_inner, double E,
+                            OBox* __restrict__ obb) {
+  for (int ci = blockIdx.x * blockDim.x + threadIdx.x; ci < 2 * n_inner; ci += gridDim.x * blockDim.x) {
+    int first, cnt;
+    child_range(nodes, ci >> 1, ci & 1, first, cnt);
+    if (cnt >= kObbWarpMin && cnt <= kObbMaxLeaves) continue;
+    OBox o;
+    if (cnt >= 2 && cnt <= kObbMaxLeaves) {
+      o = fit_obox<false>(lv32, first, cnt, E, 0);
+    } else {
       o.a0 = make_float4(1.f, 0.f, 0.f, 0.f);
       o.a1 = make_float4(0.f, 1.f, 0.f, 0.f);
       o.a2 = make_float4(0.f, 0.f, 1.f, 0.f);
       o.e = make_float4(kNoObb, kNoObb, kNoObb, 0.f);
-      if (cnt >= 2 && cnt <= kObbMaxLeaves) {
-        const float4 r4 = lv32[3 * first];
-        const double rx = r4.x, ry = r4.y, rz = r4.z;
-        double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // sums of x, y, z, xx, xy, xz, yy, yz, zz
-        for (int l = first + lane; l < first + cnt; l += 32)
-          for (int k = 0; k < 3; ++k) {
-            const float4 v = lv32[3 * l + k];
-            const double x = v.x - rx, y = v.y - ry, z = v.z - rz;
-            s[0] += x; s[1] += y; s[2] += z;
-            s[3] += x * x; s[4] += x * y; s[5] += x * z;
-            s[6] += y * y; s[7] += y * z; s[8] += z * z;
-          }
-        for (int k = 0; k < 9; ++k) s[k] = warp_sum_d(s[k]);
-        const double nv = 3.0 * cnt, mx = s[0] / nv, my = s[1] / nv, mz = s[2] / nv;
-        double C[3][3];
-        C[0][0] = s[3] / nv - mx * mx; C[0][1] = s[4] / nv - mx * my; C[0][2] = s[5] / nv - mx * mz;
-        C[1][1] = s[6] / nv - my * my; C[1][2] = s[7] / nv - my * mz; C[2][2] = s[8] / nv - mz * mz;
-        C[1][0] = C[0][1]; C[2][0] = C[0][2]; C[2][1] = C[1][2];
-        double V[3][3];
-        jacobi3(C, V);
-        float ax[3][3];
-        for (int k = 0; k < 3; ++k)
-          for (int c = 0; c < 3; ++c) ax[k][c] = (float)V[c][k];
-        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-        for (int l = first + lane; l < first + cnt; l += 32)
-          for (int k = 0; k < 3; ++k) {
-            const float4 v = lv32[3 * l + k];
-            for (int a = 0; a < 3; ++a) {  // float x float products are exact in FP64
-              const double t = (double)v.x * ax[a][0] + (double)v.y * ax[a][1] + (double)v.z * ax[a][2];
-              lo[a] = fmin(lo[a], t);
-              hi[a] = fmax(hi[a], t);
-            }
-          }
-        float ce[3], ex[3];
-        for (int a = 0; a < 3; ++a) {
-          for (int off = 16; off > 0; off >>= 1) {
-            lo[a] = fmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], off));
-            hi[a] = fmax(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], off));
-          }
-          const double c = 0.5 * (lo[a] + hi[a]);
-          ce[a] = (float)c;
-          // the FP64 sums above round by at most ~1e-15 E; the margin 1e-9 E covers them
-          ex[a] = __double2float_ru(0.5 * (hi[a] - lo[a]) + fabs(c - (double)ce[a]) + 1e-9 * E);
-        }
-        o.a0 = make_float4(ax[0][0], ax[0][1], ax[0][2], ce[0]);
-        o.a1 = make_float4(ax[1][0], ax[1][1], ax[1][2], ce[1]);
-        o.a2 = make_float4(ax[2][0], ax[2][1], ax[2][2], ce[2]);
-        o.e = make_float4(ex[0], ex[1], ex[2], 0.f);
-      }
-      if (lane == 0) obb[2 * i + side] = o;
     }
+    obb[ci] = o;
+  }
+}
+
+__global__ void k_obb_large(const BNode* __restrict__ nodes, const float4* __restrict__ lv32, int n_inner, double E,
+                            OBox* __restrict__ obb) {
+  const int lane = threadIdx.x & 31, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ci < 2 * n_inner; ci += nw) {
+    int first, cnt;
+    child_range(nodes, ci >> 1, ci & 1, first, cnt);
+    if (cnt < kObbWarpMin || cnt > kObbMaxLeaves) continue;
+    const OBox o = fit_obox<true>(lv32, first, cnt, E, lane);
+    if (lane == 0) obb[ci] = o;
   }
 }
 
@@ -400,7 +465,7 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
   ctx->mesh.ine_ready = false;
   ctx->launches = 0;
   // the previous mesh's LBVH build reads the buffers rewritten below
-  SDF_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_bvh, 0));
+  SDF_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_obb, 0));
   SDF_CUDA(ctx, cudaEventRecord(ctx->ev[4], st));
 
   double* dX;
@@ -459,8 +524,9 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
   SDF_KERNEL(ctx);
 
   // LBVH, on its own stream: only the unbounded search, the 3-nearest-vertex fallback and the
-  // adaptive rays read it, and they wait for ev_bvh; the tile lists and the fold do not, so the
-  // build overlaps the distance stage of the next call.
+  // adaptive rays read it, and they wait for ev_bvh (the unbounded search for ev_obb, which also
+  // covers the oriented boxes); the tile lists and the fold do not, so the build overlaps the
+  // distance stage of the next call.
   SDF_CUDA(ctx, cudaEventRecord(ctx->ev_mesh, st));
   cudaStream_t sb = ctx->bvh_stream;
   SDF_CUDA(ctx, cudaStreamWaitEvent(sb, ctx->ev_mesh, 0));
@@ -509,12 +575,17 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
   SDF_TRY(scratch_t(ctx, "lbox32", (size_t)n * 2, &lbox));
   k_leaf_order<<<grid_for(n, 256), 256, 0, sb>>>(leaf_prim, v32, box32, n, lv32, lbox);
   SDF_KERNEL(ctx);
+  // the rays and the 3-nearest-vertex fallback need only the tree; the unbounded searches wait for
+  // the oriented boxes as well
+  SDF_CUDA(ctx, cudaEventRecord(ctx->ev_bvh, sb));
   OBox* obb;
   const int n_inner = std::max(1, n - 1);
   SDF_TRY(scratch_t(ctx, "obb", (size_t)2 * n_inner, &obb));
-  k_obb<<<grid_for(n_inner, 8, 148 * 32), 256, 0, sb>>>(nodes, lv32, n_inner, M.E, obb);
+  k_obb_small<<<grid_for(2 * n_inner, 256), 256, 0, sb>>>(nodes, lv32, n_inner, M.E, obb);
   SDF_KERNEL(ctx);
-  SDF_CUDA(ctx, cudaEventRecord(ctx->ev_bvh, sb));
+  k_obb_large<<<grid_for(2 * n_inner, 8, 148 * 16), 256, 0, sb>>>(nodes, lv32, n_inner, M.E, obb);
+  SDF_KERNEL(ctx);
+  SDF_CUDA(ctx, cudaEventRecord(ctx->ev_obb, sb));
   unsigned long long hrho = 0;
   SDF_CUDA(ctx, cudaMemcpyAsync(&hrho, bb + 7, sizeof(hrho), cudaMemcpyDeviceToHost, st));
   SDF_CUDA(ctx, cudaEventRecord(ctx->ev[5], st));

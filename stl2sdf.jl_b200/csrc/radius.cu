@@ -605,7 +605,7 @@ int train_radius(sdfgpu_ctx* ctx, int coarse_n, int steps, int batch, float lr, 
   double* dd;
   SDF_TRY(scratch_t(ctx, "mlp_dist", (size_t)ngp, &dd));
   // the exact unbounded distances of the coarse grid (sparse nodes: one nearest-first walk per node)
-  SDF_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_bvh, 0));
+  SDF_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_obb, 0));
   SDF_TRY(run_nearest_points(ctx, g, dd));
   RadiusNorm& R = ctx->radius;
   R.c[0] = 0.5 * (o[0] + amax[0]);
