@@ -604,8 +604,8 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
         SDF_TRY(run_radius(ctx, &g, nullptr, g.ngp, R.alpha, (float)(R.beta * R.coarse_h / R.s), radius));
       }
     }
-    UnbArgs A{g, nodes, leaf_prim, v32, rec, kUnbPadRel * E, eD_abs, eD_rel, 2 * nel + 64, radius, d_dist, d_xp,
-              ctx->d_counters};
+    UnbArgs A{g, nodes, buf<LeafTri>(ctx, "ltri"), rec, kUnbPadRel * E, eD_abs, eD_rel, 2 * nel + 64, radius, d_dist,
+              d_xp, ctx->d_counters};
     A.obb = buf<OBox>(ctx, "obb");
     A.nbricks = 1;
     for (int a = 0; a < 3; ++a) {

@@ -69,6 +69,51 @@ __device__ __forceinline__ float obox_d2(float3 p, const OBox& o) {
   return fmaf(u0, u0, fmaf(u1, u1, u2 * u2));
 }
 
+// Leaf-ordered FP32 record of one triangle for the unbounded searches (mesh-local; every field
+// rounded once from its FP64 value): vertex a, edges e0 = b - a and e1 = c - a, the inverse squared
+// lengths of e0, e1 and c - b, the unit normal n and, for each edge, the unit in-plane normal m_k
+// pointing into the triangle with its offset o_k (a point of the plane lies inside when
+// (p - a).m_k >= o_k for k = 0, 1, 2).  A triangle without area has m_k = 0 and o_k = 1 and
+// reduces to its three edges.
+struct __align__(16) LeafTri {
+  float4 a;   // a.xyz, 1 / |e0|^2
+  float4 e0;  // e0.xyz, 1 / |e1|^2
+  float4 e1;  // e1.xyz, 1 / |c - b|^2
+  float4 n;   // n.xyz, triangle index (int bits)
+  float4 m0;  // edge a -> b: m0.xyz, o0 = 0
+  float4 m1;  // edge b -> c: m1.xyz, o1 = e0.m1
+  float4 m2;  // edge c -> a: m2.xyz, o2 = e1.m2
+};
+
+__device__ __forceinline__ float clamp01(float t) { return fminf(fmaxf(t, 0.f), 1.f); }
+
+// Squared distance from p to the triangle of T, without division or branch: the smallest squared
+// distance to the three edges, and the squared plane distance when p projects inside.  Every
+// rounding is relative to |w| <= d + |e| (w = p - a, d the distance, e the longest edge) or to
+// |e|, and the inside test compares physical distances to the edge lines (no barycentric
+// division), so for inputs within E of the origin the result is within about 7e-7 E + 4e-7 d of
+// the exact distance to the FP64 triangle, whatever its shape -- at least 5x inside the FP32 band
+// of the unbounded searches (4e-6 E + 4e-6 d).
+__device__ __forceinline__ float leaf_d2(float3 p, const LeafTri& T) {
+  const float wx = p.x - T.a.x, wy = p.y - T.a.y, wz = p.z - T.a.z;
+  const float t0 = clamp01(fmaf(wx, T.e0.x, fmaf(wy, T.e0.y, wz * T.e0.z)) * T.a.w);
+  const float t1 = clamp01(fmaf(wx, T.e1.x, fmaf(wy, T.e1.y, wz * T.e1.z)) * T.e0.w);
+  const float q0x = fmaf(-t0, T.e0.x, wx), q0y = fmaf(-t0, T.e0.y, wy), q0z = fmaf(-t0, T.e0.z, wz);
+  const float q1x = fmaf(-t1, T.e1.x, wx), q1y = fmaf(-t1, T.e1.y, wy), q1z = fmaf(-t1, T.e1.z, wz);
+  const float e2x = T.e1.x - T.e0.x, e2y = T.e1.y - T.e0.y, e2z = T.e1.z - T.e0.z;  // c - b
+  const float wbx = wx - T.e0.x, wby = wy - T.e0.y, wbz = wz - T.e0.z;              // p - b
+  const float t2 = clamp01(fmaf(wbx, e2x, fmaf(wby, e2y, wbz * e2z)) * T.e1.w);
+  const float q2x = fmaf(-t2, e2x, wbx), q2y = fmaf(-t2, e2y, wby), q2z = fmaf(-t2, e2z, wbz);
+  float d2 = fminf(fmaf(q0x, q0x, fmaf(q0y, q0y, q0z * q0z)),
+                   fminf(fmaf(q1x, q1x, fmaf(q1y, q1y, q1z * q1z)), fmaf(q2x, q2x, fmaf(q2y, q2y, q2z * q2z))));
+  const bool in0 = fmaf(wx, T.m0.x, fmaf(wy, T.m0.y, wz * T.m0.z)) >= T.m0.w;
+  const bool in1 = fmaf(wx, T.m1.x, fmaf(wy, T.m1.y, wz * T.m1.z)) >= T.m1.w;
+  const bool in2 = fmaf(wx, T.m2.x, fmaf(wy, T.m2.y, wz * T.m2.z)) >= T.m2.w;
+  const float dp = fmaf(wx, T.n.x, fmaf(wy, T.n.y, wz * T.n.z));
+  if (in0 && in1 && in2) d2 = fminf(d2, dp * dp);
+  return d2;
+}
+
 // Squared distance from p to the box [lo, hi].
 __device__ __forceinline__ float box_d2(float3 p, float3 lo, float3 hi) {
   const float dx = fmaxf(fmaxf(lo.x - p.x, p.x - hi.x), 0.f);

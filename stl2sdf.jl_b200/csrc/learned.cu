@@ -12,8 +12,6 @@ namespace {
 
 struct LearnArgs {
   UnbArgs u;
-  const float4* lv32;  // leaf-ordered FP32 vertices (3 per leaf)
-  const float4* lbox;  // leaf-ordered FP32 boxes (2 per leaf; lo.w = triangle index)
 };
 
 
@@ -61,8 +59,9 @@ __device__ bool point_search(const LearnArgs& LA, const d3& p, const float3& p32
       const float b = bound() + A.pad;
       if (!(dc <= b * b)) continue;
       const int leaf = c & 0x7fffffff;
-      const int prim = __float_as_int(LA.lbox[2 * leaf].w);
-      const float D = sqrtf(pt_tri_d2(p32, f3(LA.lv32[3 * leaf]), f3(LA.lv32[3 * leaf + 1]), f3(LA.lv32[3 * leaf + 2])));
+      const LeafTri T = A.ltri[leaf];
+      const int prim = __float_as_int(T.n.w);
+      const float D = sqrtf(leaf_d2(p32, T));
       if (D > bound()) continue;
       if (kExact) {
         step64_call(A.rec, prim, p, m64, proj);
@@ -160,8 +159,7 @@ LearnArgs point_args(sdfgpu_ctx* ctx, const GridP& g, double* d_dist) {
   A.max_visits = 2 * ctx->mesh.nel + 64;
   A.dist = d_dist;
   A.counters = ctx->d_counters;
-  LA.lv32 = buf<float4>(ctx, "lv32");
-  LA.lbox = buf<float4>(ctx, "lbox32");
+  A.ltri = buf<LeafTri>(ctx, "ltri");
   return LA;
 }
 

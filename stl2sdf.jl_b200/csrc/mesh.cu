@@ -237,21 +237,58 @@ __global__ void k_single_root(const float4* __restrict__ box32, BNode* nodes, in
   leaf_prim[0] = 0;
 }
 
-// Leaf-ordered copies for the learned-radius search, which reads runs of consecutive leaves: the
-// FP32 vertices (3 x float4, as v32) and the outward-rounded box (2 x float4, as box32) of the
-// triangle at each sorted leaf; the box's lo.w carries the triangle's index.
+// Leaf-ordered copies for the unbounded searches and the oriented-box fit, which read the
+// triangles of runs of consecutive leaves: the FP32 vertices (3 x float4, as v32) and the LeafTri
+// record, both of the triangle at each sorted leaf.  The record's fields are computed in FP64 from
+// the triangle's vertices (mesh-local) and rounded once.
 __global__ void k_leaf_order(const int32_t* __restrict__ leaf_prim, const float4* __restrict__ v32,
-                             const float4* __restrict__ box32, int n, float4* __restrict__ lv32,
-                             float4* __restrict__ lbox) {
+                             const TriRec64* __restrict__ rec, int n, double cx, double cy, double cz,
+                             float4* __restrict__ lv32, LeafTri* __restrict__ ltri) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int prim = leaf_prim[i];
     lv32[3 * i] = v32[3 * prim];
     lv32[3 * i + 1] = v32[3 * prim + 1];
     lv32[3 * i + 2] = v32[3 * prim + 2];
-    float4 lo = box32[2 * prim];
-    lo.w = __int_as_float(prim);
-    lbox[2 * i] = lo;
-    lbox[2 * i + 1] = box32[2 * prim + 1];
+    const double* v = rec[prim].v;
+    const double ax = v[0] - cx, ay = v[1] - cy, az = v[2] - cz;
+    const double e0[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]};
+    const double e1[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
+    const double e2[3] = {v[6] - v[3], v[7] - v[4], v[8] - v[5]};
+    const double l0 = e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2];
+    const double l1 = e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2];
+    const double l2 = e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2];
+    const double nx = e0[1] * e1[2] - e0[2] * e1[1], ny = e0[2] * e1[0] - e0[0] * e1[2], nz = e0[0] * e1[1] - e0[1] * e1[0];
+    const double nn = nx * nx + ny * ny + nz * nz;
+    LeafTri T;
+    T.a = make_float4((float)ax, (float)ay, (float)az, (float)(1.0 / l0));
+    T.e0 = make_float4((float)e0[0], (float)e0[1], (float)e0[2], (float)(1.0 / l1));
+    T.e1 = make_float4((float)e1[0], (float)e1[1], (float)e1[2], (float)(1.0 / l2));
+    if (nn > 1e-20 * l0 * l1) {
+      const double rn = 1.0 / sqrt(nn), un[3] = {nx * rn, ny * rn, nz * rn};
+      // inward in-plane edge normals: n x (edge direction), edges a->b, b->c, c->a
+      const double* ed[3] = {e0, e2, e1};
+      const double sg[3] = {1.0, 1.0, -1.0};
+      double m[3][3];
+      for (int k = 0; k < 3; ++k) {
+        const double* d = ed[k];
+        const double mx = sg[k] * (un[1] * d[2] - un[2] * d[1]), my = sg[k] * (un[2] * d[0] - un[0] * d[2]),
+                     mz = sg[k] * (un[0] * d[1] - un[1] * d[0]);
+        const double r = 1.0 / sqrt(mx * mx + my * my + mz * mz);
+        m[k][0] = mx * r; m[k][1] = my * r; m[k][2] = mz * r;
+      }
+      T.n = make_float4((float)un[0], (float)un[1], (float)un[2], __int_as_float(prim));
+      T.m0 = make_float4((float)m[0][0], (float)m[0][1], (float)m[0][2], 0.f);
+      T.m1 = make_float4((float)m[1][0], (float)m[1][1], (float)m[1][2],
+                         (float)(e0[0] * m[1][0] + e0[1] * m[1][1] + e0[2] * m[1][2]));
+      T.m2 = make_float4((float)m[2][0], (float)m[2][1], (float)m[2][2],
+                         (float)(e1[0] * m[2][0] + e1[1] * m[2][1] + e1[2] * m[2][2]));
+    } else {  // no area: the edges alone
+      T.n = make_float4(0.f, 0.f, 0.f, __int_as_float(prim));
+      T.m0 = make_float4(0.f, 0.f, 0.f, 1.f);
+      T.m1 = make_float4(0.f, 0.f, 0.f, 1.f);
+      T.m2 = make_float4(0.f, 0.f, 0.f, 1.f);
+    }
+    ltri[i] = T;
   }
 }
 
@@ -570,10 +607,12 @@ int mesh_upload_and_build(sdfgpu_ctx* ctx, const double* X, int64_t nnp, const i
     k_refit<<<grid_for(n, 256), 256, 0, sb>>>(keys2, box32, n, nodes, int_parent, leaf_parent, flags, leaf_prim);
     SDF_KERNEL(ctx);
   }
-  float4 *lv32, *lbox;
+  float4* lv32;
+  LeafTri* ltri;
   SDF_TRY(scratch_t(ctx, "lv32", (size_t)n * 3, &lv32));
-  SDF_TRY(scratch_t(ctx, "lbox32", (size_t)n * 2, &lbox));
-  k_leaf_order<<<grid_for(n, 256), 256, 0, sb>>>(leaf_prim, v32, box32, n, lv32, lbox);
+  SDF_TRY(scratch_t(ctx, "ltri", (size_t)n, &ltri));
+  k_leaf_order<<<grid_for(n, 256), 256, 0, sb>>>(leaf_prim, v32, rec, n, M.center[0], M.center[1], M.center[2], lv32,
+                                                 ltri);
   SDF_KERNEL(ctx);
   // the rays and the 3-nearest-vertex fallback need only the tree; the unbounded searches wait for
   // the oriented boxes as well

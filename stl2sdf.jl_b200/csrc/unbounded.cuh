@@ -40,8 +40,7 @@ constexpr int kKeep = 8;         // per-lane triangles kept inside the FP32 band
 struct UnbArgs {
   GridP g;
   const BNode* nodes;
-  const int32_t* leaf_prim;
-  const float4* v32;
+  const LeafTri* ltri;  // leaf-ordered FP32 triangle records
   const TriRec64* rec;
   float pad;
   float eD_abs, eD_rel;
@@ -188,8 +187,9 @@ __device__ bool warp_search(const UnbArgs& A, int* stack, int lane, int rep, con
       const int c = q == 0 ? cn : cf;
       const bool want = q == 0 ? wn : wf;
       if (!(c & kLeafBit) || (q == 0 ? mn : mfar) == 0u) continue;
-      const int prim = A.leaf_prim[c & 0x7fffffff];
-      const float D = sqrtf(pt_tri_d2(p32, f3(A.v32[3 * prim]), f3(A.v32[3 * prim + 1]), f3(A.v32[3 * prim + 2])));
+      const LeafTri T = A.ltri[c & 0x7fffffff];
+      const int prim = __float_as_int(T.n.w);
+      const float D = sqrtf(leaf_d2(p32, T));
       if (kExact) {
         const float mf = (float)m64;
         if (want && D <= fminf(r0, mf + A.eD_abs + A.eD_rel * mf)) {
