@@ -74,6 +74,14 @@ struct GridP {
 __device__ __forceinline__ d3 gnode(const GridP& g, int64_t i, int64_t j, int64_t k) {
   return node_coord(g.o, g.h, i, j, k + g.k0);
 }
+// Centre of warp brick (bx, by, bz) of b[0] x b[1] x b[2] nodes, clipped to the grid: the midpoint of
+// its first and last nodes (FP64).  The learned radius is predicted there, once per brick.
+__device__ __forceinline__ d3 brick_center(const GridP& g, const int32_t b[3], int64_t bx, int64_t by, int64_t bz) {
+  const d3 lo = gnode(g, bx * b[0], by * b[1], bz * b[2]);
+  const d3 hi = gnode(g, min(bx * b[0] + b[0] - 1, g.N[0]), min(by * b[1] + b[1] - 1, g.N[1]),
+                      min(bz * b[2] + b[2] - 1, g.N[2]));
+  return {0.5 * (lo.x + hi.x), 0.5 * (lo.y + hi.y), 0.5 * (lo.z + hi.z)};
+}
 // Global index along axis a of local index idx.
 __host__ __device__ __forceinline__ int64_t gidx(const GridP& g, int a, int64_t idx) {
   return a == 2 ? idx + g.k0 : idx;
@@ -275,7 +283,8 @@ int cub_scan_i32(sdfgpu_ctx* ctx, const int32_t* in, int32_t* out, int64_t n, cu
 int train_radius(sdfgpu_ctx* ctx, int coarse_n, int steps, int batch, float lr, uint64_t seed, float* final_loss);
 int set_radius_params(sdfgpu_ctx* ctx, const float* params, const double norm[4]);
 int get_radius_params(sdfgpu_ctx* ctx, float* params, double norm[4]);
-int run_radius(sdfgpu_ctx* ctx, const GridP* g, const float* d_pts, int64_t count, float alpha, float beta, float* d_out);
+int run_radius(sdfgpu_ctx* ctx, const GridP* g, const float* d_pts, int64_t count, float alpha, float beta, float* d_out,
+               const int32_t* brick = nullptr);
 int mlp_eval_host(sdfgpu_ctx* ctx, const float* params, const float* xn, const float* target, int64_t B, float* yhat,
                   float* loss, float* grad);
 int cub_scan_i64(sdfgpu_ctx* ctx, const int64_t* in, int64_t* out, int64_t n);

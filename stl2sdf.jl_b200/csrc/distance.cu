@@ -491,10 +491,10 @@ __global__ void k_knn_fallback(KnnArgs A) {
 }
 
 // True nearest triangle of every node (no clamp), one warp per brick of 32 nodes.  With a learned
-// radius r the first search of each lane is bounded by r; a minimum certainly <= r is exact (every
-// nearer triangle lies within r and was visited), and the lanes without one search again without
-// the bound, keeping what they found.  Lanes whose band overflowed search once more with FP64
-// steps bounded by the band.
+// radius (predicted at the brick centre c, r = rc + |p - c| for node p) the first search of each
+// lane is bounded by r; a minimum certainly <= r is exact (every nearer triangle lies within r and
+// was visited), and the lanes without one search again without the bound, keeping what they found.
+// Lanes whose band overflowed search once more with FP64 steps bounded by the band.
 __global__ void __launch_bounds__(kUnbThreads, 4) k_unbounded(UnbArgs A) {
   __shared__ int s_stack[kUnbWarps][kWarpStack];
   __shared__ int s_keep_t[kKeep * kUnbThreads];
@@ -527,7 +527,13 @@ __global__ void __launch_bounds__(kUnbThreads, 4) k_unbounded(UnbArgs A) {
     d3 proj = {0.0, 0.0, 0.0};
     bool ok;
     if (A.radius) {
-      const float r = valid ? A.radius[lin] : 0.f;
+      // the brick's radius plus the node's distance from the brick centre where it was predicted
+      float r = 0.f;
+      if (valid) {
+        const d3 c = brick_center(g, A.b, bx, by, bz);
+        const double dx = p.x - c.x, dy = p.y - c.y, dz = p.z - c.z;
+        r = (float)((double)A.radius[brick] + sqrt(dx * dx + dy * dy + dz * dz));
+      }
       ok = warp_search<false, kUnbThreads>(A, stack, lane, rep, p, p32, valid, r, L, m64, proj, fp64, visits);
       const bool certified = valid && L.m < INFINITY && L.m + A.eD_abs + A.eD_rel * L.m <= r;
       if (valid && certified) ++cert;
@@ -593,18 +599,7 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
 
   if (mode == SDFGPU_MODE_UNBOUNDED) {
     SDF_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_obb, 0));  // the search walks the LBVH and its oriented boxes
-    float* radius = nullptr;
-    if (use_learned) {
-      // r = (dhat (1 + alpha) + beta * coarse spacing / s) s: a margin for the network's error and
-      // for the interpolation between the training nodes
-      // (alpha = +inf: every radius infinite, the same search without the network's bound)
-      const RadiusNorm& R = ctx->radius;
-      if (!std::isinf(R.alpha)) {
-        SDF_TRY(scratch_t(ctx, "radius", (size_t)g.ngp, &radius));
-        SDF_TRY(run_radius(ctx, &g, nullptr, g.ngp, R.alpha, (float)(R.beta * R.coarse_h / R.s), radius));
-      }
-    }
-    UnbArgs A{g, nodes, buf<LeafTri>(ctx, "ltri"), rec, kUnbPadRel * E, eD_abs, eD_rel, 2 * nel + 64, radius, d_dist,
+    UnbArgs A{g, nodes, buf<LeafTri>(ctx, "ltri"), rec, kUnbPadRel * E, eD_abs, eD_rel, 2 * nel + 64, nullptr, d_dist,
               d_xp, ctx->d_counters};
     A.obb = buf<OBox>(ctx, "obb");
     A.nbricks = 1;
@@ -612,6 +607,19 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
       A.b[a] = ctx->brick[a];
       A.nb[a] = cdiv(g.n[a], A.b[a]);
       A.nbricks *= A.nb[a];
+    }
+    if (use_learned) {
+      // the network's radius at each brick centre c, rc = (dhat (1 + alpha) + beta * coarse spacing
+      // / s) s (a margin for the network's error and for the interpolation between its training
+      // nodes); a node p of the brick searches within rc + |p - c| (k_unbounded).  alpha = +inf:
+      // no radius, the same search without the network's bound.
+      const RadiusNorm& R = ctx->radius;
+      if (!std::isinf(R.alpha)) {
+        float* radius;
+        SDF_TRY(scratch_t(ctx, "radius", (size_t)A.nbricks, &radius));
+        SDF_TRY(run_radius(ctx, &g, nullptr, A.nbricks, R.alpha, (float)(R.beta * R.coarse_h / R.s), radius, A.b));
+        A.radius = radius;
+      }
     }
     SDF_MARK(ctx, T_TILES);
     // one resident wave of CTAs draining the brick queue

@@ -431,6 +431,8 @@ __global__ void k_train_reduce(const float* __restrict__ partial, int nparts, in
 struct RadiusArgs {
   GridP g;          // grid of the query (ngp nodes) -- or npts explicit normalised points
   const float* pts; // nullable: B x 3 normalised points instead of grid nodes
+  int32_t b[3];     // b[0] > 0: the query is the centre of each warp brick of b nodes (nb per axis)
+  int64_t nb[3];
   int64_t count;
   double cx, cy, cz, s;
   float alpha, beta;  // r = (dhat (1 + alpha) + beta) * s; alpha < 0: write dhat itself
@@ -463,8 +465,12 @@ __global__ void __launch_bounds__(128) k_radius(RadiusArgs A) {
       if (A.pts) {
         x0 = A.pts[3 * q]; x1 = A.pts[3 * q + 1]; x2 = A.pts[3 * q + 2];
       } else {
-        const int64_t i = q % G.n[0], j = (q / G.n[0]) % G.n[1], k = q / (G.n[0] * G.n[1]);
-        const d3 p = node_coord(G.o, G.h, i, j, k);
+        d3 p;
+        if (A.b[0] > 0) {
+          p = brick_center(G, A.b, q % A.nb[0], (q / A.nb[0]) % A.nb[1], q / (A.nb[0] * A.nb[1]));
+        } else {
+          p = gnode(G, q % G.n[0], (q / G.n[0]) % G.n[1], q / (G.n[0] * G.n[1]));
+        }
         x0 = (float)((p.x - A.cx) / A.s); x1 = (float)((p.y - A.cy) / A.s); x2 = (float)((p.z - A.cz) / A.s);
       }
     }
@@ -701,7 +707,8 @@ int get_radius_params(sdfgpu_ctx* ctx, float* params, double norm[4]) {
 }
 
 // Radii (or raw dhat when alpha < 0) of the grid nodes, or of explicit normalised points.
-int run_radius(sdfgpu_ctx* ctx, const GridP* g, const float* d_pts, int64_t count, float alpha, float beta, float* d_out) {
+int run_radius(sdfgpu_ctx* ctx, const GridP* g, const float* d_pts, int64_t count, float alpha, float beta, float* d_out,
+               const int32_t* brick) {
   const RadiusNorm& R = ctx->radius;
   if (!R.trained) return fail(ctx, SDFGPU_ERR_INVALID_ARGUMENT, "no radius network: call sdfgpu_train_radius first");
   RadiusArgs A;
@@ -709,6 +716,10 @@ int run_radius(sdfgpu_ctx* ctx, const GridP* g, const float* d_pts, int64_t coun
   else std::memset(&A.g, 0, sizeof(A.g));
   A.pts = d_pts;
   A.count = count;
+  for (int a = 0; a < 3; ++a) {
+    A.b[a] = brick ? brick[a] : 0;
+    A.nb[a] = brick && g ? cdiv(g->n[a], brick[a]) : 0;
+  }
   A.cx = R.c[0]; A.cy = R.c[1]; A.cz = R.c[2]; A.s = R.s;
   A.alpha = alpha;
   A.beta = beta;

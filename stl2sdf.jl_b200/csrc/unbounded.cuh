@@ -45,7 +45,7 @@ struct UnbArgs {
   float pad;
   float eD_abs, eD_rel;
   int64_t max_visits;
-  const float* radius;  // learned radius per node (nullable)
+  const float* radius;  // learned radius per brick, at its centre (nullable)
   double* dist;
   double* xp;
   int64_t* counters;
