@@ -495,6 +495,9 @@ __global__ void k_knn_fallback(KnnArgs A) {
 // lane is bounded by r; a minimum certainly <= r is exact (every nearer triangle lies within r and
 // was visited), and the lanes without one search again without the bound, keeping what they found.
 // Lanes whose band overflowed search once more with FP64 steps bounded by the band.
+// kRadius: A.radius is set (the learned mode); a separate instantiation, so the plain search keeps
+// its own register allocation.
+template <bool kRadius>
 __global__ void __launch_bounds__(kUnbThreads, 4) k_unbounded(UnbArgs A) {
   __shared__ int s_stack[kUnbWarps][kWarpStack];
   __shared__ int s_keep_t[kKeep * kUnbThreads];
@@ -525,24 +528,30 @@ __global__ void __launch_bounds__(kUnbThreads, 4) k_unbounded(UnbArgs A) {
     }
     double m64 = kBig;
     d3 proj = {0.0, 0.0, 0.0};
-    bool ok;
-    if (A.radius) {
-      // the brick's radius plus the node's distance from the brick centre where it was predicted
-      float r = 0.f;
+    bool ok = true;
+    // kRadius: the first pass is bounded by r, the brick's radius plus the node's distance from the
+    // brick centre where it was predicted; lanes not certified by it take a second, unbounded pass
+    float r = INFINITY;
+    if (kRadius) {
+      r = 0.f;
       if (valid) {
         const d3 c = brick_center(g, A.b, bx, by, bz);
         const double dx = p.x - c.x, dy = p.y - c.y, dz = p.z - c.z;
         r = (float)((double)A.radius[brick] + sqrt(dx * dx + dy * dy + dz * dz));
       }
-      ok = warp_search<false, kUnbThreads>(A, stack, lane, rep, p, p32, valid, r, L, m64, proj, fp64, visits);
-      const bool certified = valid && L.m < INFINITY && L.m + A.eD_abs + A.eD_rel * L.m <= r;
-      if (valid && certified) ++cert;
-      if (valid && !certified) ++fallback;
-      if (ok && __any_sync(0xffffffffu, valid && !certified))
-        ok = warp_search<false, kUnbThreads>(A, stack, lane, rep, p, p32, valid && !certified, INFINITY, L, m64, proj, fp64,
-                                visits);
-    } else {
-      ok = warp_search<false, kUnbThreads>(A, stack, lane, rep, p, p32, valid, INFINITY, L, m64, proj, fp64, visits);
+    }
+    bool searching = valid;
+#pragma unroll 1
+    for (int pass = 0; pass < (kRadius ? 2 : 1); ++pass) {
+      if (pass == 1) {
+        const bool certified = valid && L.m < INFINITY && L.m + A.eD_abs + A.eD_rel * L.m <= r;
+        if (valid && certified) ++cert;
+        if (valid && !certified) ++fallback;
+        searching = valid && !certified;
+        if (!ok || !__any_sync(0xffffffffu, searching)) break;
+      }
+      ok = warp_search<false, kUnbThreads>(A, stack, lane, rep, p, p32, searching, pass == 0 ? r : INFINITY, L, m64,
+                                           proj, fp64, visits);
     }
     const bool over = valid && L.overflow;
     if (ok && __any_sync(0xffffffffu, over))
@@ -626,9 +635,10 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
     SDF_TRY(scratch_t(ctx, "brick_next", 1, &A.next));
     SDF_CUDA(ctx, cudaMemsetAsync(A.next, 0, sizeof(unsigned long long), st));
     int per_sm = 0, sms = 148;
-    SDF_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_unbounded, kUnbWarps * 32, 0));
+    const auto kern = A.radius ? k_unbounded<true> : k_unbounded<false>;
+    SDF_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kUnbWarps * 32, 0));
     SDF_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    k_unbounded<<<grid_for(A.nbricks, kUnbWarps, (int64_t)sms * std::max(per_sm, 1)), kUnbWarps * 32, 0, st>>>(A);
+    kern<<<grid_for(A.nbricks, kUnbWarps, (int64_t)sms * std::max(per_sm, 1)), kUnbWarps * 32, 0, st>>>(A);
     SDF_KERNEL(ctx);
     SDF_MARK(ctx, T_FOLD);
     return 0;
