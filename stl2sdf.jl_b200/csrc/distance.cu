@@ -491,15 +491,22 @@ __global__ void k_knn_fallback(KnnArgs A) {
 }
 
 // True nearest triangle of every node (no clamp), one warp per brick of 32 nodes.  With a learned
-// radius (predicted at the brick centre c, r = rc + |p - c| for node p) the first search of each
-// lane is bounded by r; a minimum certainly <= r is exact (every nearer triangle lies within r and
-// was visited), and the lanes without one search again without the bound, keeping what they found.
-// Lanes whose band overflowed search once more with FP64 steps bounded by the band.
-// kRadius: A.radius is set (the learned mode); a separate instantiation, so the plain search keeps
-// its own register allocation.
-template <bool kRadius>
+// radius (predicted at the brick centre c, r = rc + |p - c| for node p) each lane's search starts
+// bounded by r, and a lane that finds a triangle below r is exact (below).  Lanes whose band
+// overflowed search once more with FP64 steps bounded by the band.
+// kMode kUnbPlain: every brick, unbounded.  kUnbRadius (the learned mode, A.radius set): one pass
+// that starts each lane's minimum at its radius r; a brick with a lane that the pass does not
+// certify is appended to A.redo and left unwritten.  kUnbListed: the plain search over the bricks
+// listed in A.bricks (the learned mode's second launch).
+constexpr int kUnbPlain = 0, kUnbRadius = 1, kUnbListed = 2;
+template <int kMode>
 __global__ void __launch_bounds__(kUnbThreads, 4) k_unbounded(UnbArgs A) {
+  constexpr bool kRadius = kMode == kUnbRadius, kListed = kMode == kUnbListed;
   __shared__ int s_stack[kUnbWarps][kWarpStack];
+  // kRadius: each lane's radius and the warp's certified / fallback counts live in shared memory,
+  // so the traversal loop keeps the plain search's registers
+  __shared__ float s_r[kRadius ? kUnbThreads : 1];
+  __shared__ unsigned s_cf[kRadius ? kUnbWarps : 1][2];
   __shared__ int s_keep_t[kKeep * kUnbThreads];
   __shared__ float s_keep_d[kKeep * kUnbThreads];
   const GridP& g = A.g;
@@ -507,8 +514,11 @@ __global__ void __launch_bounds__(kUnbThreads, 4) k_unbounded(UnbArgs A) {
   int* stack = s_stack[w];
   const int lx = lane % A.b[0], ly = (lane / A.b[0]) % A.b[1], lz = lane / (A.b[0] * A.b[1]);
   const int rep = A.b[0] / 2 + A.b[0] * (A.b[1] / 2 + A.b[1] * (A.b[2] / 2));
-  int64_t fp64 = 0, cert = 0, fallback = 0, errs = 0, visits = 0;
-  for (int64_t brick = next_brick(A, lane); brick < A.nbricks; brick = next_brick(A, lane)) {
+  int64_t fp64 = 0, errs = 0, visits = 0;
+  if (kRadius && lane == 0) s_cf[w][0] = s_cf[w][1] = 0u;
+  const int64_t total = kListed ? (int64_t)*A.bricks_n : A.nbricks;
+  for (int64_t q = next_brick(A, lane); q < total; q = next_brick(A, lane)) {
+    const int64_t brick = kListed ? A.bricks[q] : q;
     const int64_t bx = brick % A.nb[0], by = (brick / A.nb[0]) % A.nb[1], bz = brick / (A.nb[0] * A.nb[1]);
     const int64_t i = bx * A.b[0] + lx, j = by * A.b[1] + ly, k = bz * A.b[2] + lz;
     const bool valid = i <= g.N[0] && j <= g.N[1] && k <= g.N[2];
@@ -528,30 +538,34 @@ __global__ void __launch_bounds__(kUnbThreads, 4) k_unbounded(UnbArgs A) {
     }
     double m64 = kBig;
     d3 proj = {0.0, 0.0, 0.0};
-    bool ok = true;
-    // kRadius: the first pass is bounded by r, the brick's radius plus the node's distance from the
-    // brick centre where it was predicted; lanes not certified by it take a second, unbounded pass
-    float r = INFINITY;
-    if (kRadius) {
-      r = 0.f;
-      if (valid) {
-        const d3 c = brick_center(g, A.b, bx, by, bz);
-        const double dx = p.x - c.x, dy = p.y - c.y, dz = p.z - c.z;
-        r = (float)((double)A.radius[brick] + sqrt(dx * dx + dy * dy + dz * dz));
-      }
+    // kRadius: the lane's FP32 minimum starts at r -- the brick's radius plus the node's distance
+    // from the brick centre where it was predicted -- as if a triangle lay there, and the pass is the
+    // plain search from that state.  A triangle with FP32 distance below r is never pruned (its box
+    // bound is below r, and every bound of the lane stays >= its minimum), so a lane that ends below
+    // r holds the true FP32 minimum and its band, exactly as the unbounded search would: it is
+    // certified.  A brick with a lane left at r goes to the plain search of the listed bricks.
+    if (kRadius && valid) {
+      const d3 c = brick_center(g, A.b, bx, by, bz);
+      const double dx = p.x - c.x, dy = p.y - c.y, dz = p.z - c.z;
+      L.m = (float)((double)A.radius[brick] + sqrt(dx * dx + dy * dy + dz * dz));
+      s_r[threadIdx.x] = L.m;
     }
-    bool searching = valid;
-#pragma unroll 1
-    for (int pass = 0; pass < (kRadius ? 2 : 1); ++pass) {
-      if (pass == 1) {
-        const bool certified = valid && L.m < INFINITY && L.m + A.eD_abs + A.eD_rel * L.m <= r;
-        if (valid && certified) ++cert;
-        if (valid && !certified) ++fallback;
-        searching = valid && !certified;
-        if (!ok || !__any_sync(0xffffffffu, searching)) break;
+    bool ok = warp_search<false, kUnbThreads>(A, stack, lane, rep, p, p32, valid, INFINITY, L, m64, proj, fp64, visits);
+    if (kRadius && ok) {
+      const bool certified = valid && L.m < s_r[threadIdx.x];
+      const unsigned nc = __popc(__ballot_sync(0xffffffffu, valid && certified));
+      const unsigned nf = __popc(__ballot_sync(0xffffffffu, valid && !certified));
+      if (lane == 0) {
+        s_cf[w][0] += nc;
+        s_cf[w][1] += nf;
       }
-      ok = warp_search<false, kUnbThreads>(A, stack, lane, rep, p, p32, searching, pass == 0 ? r : INFINITY, L, m64,
-                                           proj, fp64, visits);
+      if (nf) {  // the whole brick again, unbounded
+        if (lane == 0) {  // lane 0 stands on the brick's first node (always inside the grid)
+          const int64_t i0 = lin % g.n[0], j0 = (lin / g.n[0]) % g.n[1], k0 = lin / (g.n[0] * g.n[1]);
+          A.redo[atomicAdd(A.redo_n, 1ULL)] = i0 / A.b[0] + A.nb[0] * (j0 / A.b[1] + A.nb[1] * (k0 / A.b[2]));
+        }
+        continue;
+      }
     }
     const bool over = valid && L.overflow;
     if (ok && __any_sync(0xffffffffu, over))
@@ -567,15 +581,11 @@ __global__ void __launch_bounds__(kUnbThreads, 4) k_unbounded(UnbArgs A) {
       }
     }
   }
-  for (int off = 16; off > 0; off >>= 1) {
-    fp64 += __shfl_down_sync(0xffffffffu, fp64, off);
-    cert += __shfl_down_sync(0xffffffffu, cert, off);
-    fallback += __shfl_down_sync(0xffffffffu, fallback, off);
-  }
+  for (int off = 16; off > 0; off >>= 1) fp64 += __shfl_down_sync(0xffffffffu, fp64, off);
   if (lane == 0) {
     if (fp64) count_add(A.counters, C_FP64, fp64);
-    if (cert) count_add(A.counters, C_CERTIFIED, cert);
-    if (fallback) count_add(A.counters, C_UNB_FALLBACK, fallback);
+    if (kRadius && s_cf[w][0]) count_add(A.counters, C_CERTIFIED, s_cf[w][0]);
+    if (kRadius && s_cf[w][1]) count_add(A.counters, C_UNB_FALLBACK, s_cf[w][1]);
     if (errs) count_add(A.counters, C_ERR_STACK, errs);
     if (visits) count_add(A.counters, C_VISITS, visits);
   }
@@ -631,14 +641,29 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
       }
     }
     SDF_MARK(ctx, T_TILES);
-    // one resident wave of CTAs draining the brick queue
-    SDF_TRY(scratch_t(ctx, "brick_next", 1, &A.next));
-    SDF_CUDA(ctx, cudaMemsetAsync(A.next, 0, sizeof(unsigned long long), st));
+    // one resident wave of CTAs draining the brick queue: queue heads of the two launches and the
+    // count of bricks handed from the bounded to the plain search, zeroed together
+    unsigned long long* heads;
+    SDF_TRY(scratch_t(ctx, "brick_next", 3, &heads));
+    SDF_CUDA(ctx, cudaMemsetAsync(heads, 0, 3 * sizeof(unsigned long long), st));
     int per_sm = 0, sms = 148;
-    const auto kern = A.radius ? k_unbounded<true> : k_unbounded<false>;
-    SDF_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kUnbWarps * 32, 0));
+    SDF_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_unbounded<kUnbPlain>, kUnbWarps * 32, 0));
     SDF_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    kern<<<grid_for(A.nbricks, kUnbWarps, (int64_t)sms * std::max(per_sm, 1)), kUnbWarps * 32, 0, st>>>(A);
+    const unsigned grid = grid_for(A.nbricks, kUnbWarps, (int64_t)sms * std::max(per_sm, 1));
+    A.next = heads;
+    if (A.radius) {
+      SDF_TRY(scratch_t(ctx, "brick_redo", (size_t)A.nbricks, &A.redo));
+      A.redo_n = heads + 2;
+      k_unbounded<kUnbRadius><<<grid, kUnbWarps * 32, 0, st>>>(A);
+      SDF_KERNEL(ctx);
+      A.radius = nullptr;  // the listed bricks (usually none), with the plain search
+      A.bricks = A.redo;
+      A.bricks_n = A.redo_n;
+      A.next = heads + 1;
+      k_unbounded<kUnbListed><<<grid, kUnbWarps * 32, 0, st>>>(A);
+    } else {
+      k_unbounded<kUnbPlain><<<grid, kUnbWarps * 32, 0, st>>>(A);
+    }
     SDF_KERNEL(ctx);
     SDF_MARK(ctx, T_FOLD);
     return 0;

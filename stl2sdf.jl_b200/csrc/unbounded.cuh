@@ -54,6 +54,10 @@ struct UnbArgs {
   int64_t nbricks;
   unsigned long long* next;  // brick queue: warps take the next brick with one atomic (zeroed per launch)
   const OBox* obb;           // oriented boxes of the LBVH children (obb[2 node + side])
+  const int64_t* bricks = nullptr;               // nullable: search only these bricks ...
+  const unsigned long long* bricks_n = nullptr;  // ... this many (read on the device)
+  int64_t* redo = nullptr;                       // the radius-bounded search lists here the bricks ...
+  unsigned long long* redo_n = nullptr;          // ... it did not certify (a counter zeroed per launch)
 };
 
 // FP32 margin of every box test of the unbounded searches, as a multiple of the frame's scale E:
