@@ -100,7 +100,8 @@ def test_blobs256_unbounded_and_learned(gpu_ctx, blobs256):
     """Plain unbounded and learned-radius searches on the full 256-node grid: identical at every
     node, equal to the oracle on 2,000 uniform and 2,000 near-surface nodes; the trained network
     certifies most nodes.  The printed times show what the network gains: on this mesh the learned
-    search runs at the plain search's speed (the seeded search without the network is as fast)."""
+    search runs within a few percent of the plain search (the radius prunes under 1% of the LBVH
+    visits)."""
     X, IEN, g = blobs256
     gpu_ctx.set_mesh(X, IEN)
     clamped, _ = gpu_ctx.distances(g["origin"], g["h"], g["N"], 1)
