@@ -110,10 +110,11 @@ struct LaneBest {
   float* d;       // shared: their FP32 distances
 };
 
-__device__ __forceinline__ float band_of(const UnbArgs& A, float m) { return m + 2.f * (A.eD_abs + A.eD_rel * m); }
+template <class P>
+__device__ __forceinline__ float band_of(const P& A, float m) { return m + 2.f * (A.eD_abs + A.eD_rel * m); }
 
-template <int S>
-__device__ __forceinline__ void lane_offer(const UnbArgs& A, LaneBest& L, float D, int tri) {
+template <int S, class P>
+__device__ __forceinline__ void lane_offer(const P& A, LaneBest& L, float D, int tri) {
   if (D < L.m) {
     L.m = D;
     const float bd = band_of(A, D);
@@ -148,8 +149,8 @@ __device__ __forceinline__ void lane_offer(const UnbArgs& A, LaneBest& L, float 
 // lane's bound runs the FP64 step at once (used with a tight r0 for lanes whose band overflowed);
 // otherwise leaves only feed the lane's FP32 band.  Returns false when the visit or stack bound is
 // exceeded.
-template <bool kExact, int S>
-__device__ bool warp_search(const UnbArgs& A, int* stack, int lane, int rep, const d3& p, const float3& p32,
+template <bool kExact, int S, class P>
+__device__ bool warp_search(const P& A, int* stack, int lane, int rep, const d3& p, const float3& p32,
                             bool active, float r0, LaneBest& L, double& m64, d3& proj, int64_t& fp64,
                             int64_t& visits_out) {
   int sp = 1;
@@ -221,6 +222,45 @@ __device__ bool warp_search(const UnbArgs& A, int* stack, int lane, int rep, con
   __syncwarp();
   visits_out += visits;
   return ok;
+}
+
+// The FP32 pass of the packet search as one out-of-line function, shared by every instantiation of
+// k_unbounded: the hot loop is compiled once, with its own register allocation, whatever the
+// calling kernel keeps live around it.  Its inputs come by value (SearchP: the fields the pass
+// reads) and its results go back by value, so nothing of the lane's state sits in local memory.
+struct SearchP {
+  const BNode* nodes;
+  const OBox* obb;
+  const LeafTri* ltri;
+  const TriRec64* rec;  // not read by the FP32 pass
+  float pad, eD_abs, eD_rel;
+  int64_t max_visits;
+};
+struct SearchOut {
+  float m;         // the lane's FP32 minimum at the end
+  bool overflow;   // its band overflowed
+  bool ok;         // the visit and stack bounds held
+  int64_t visits;
+};
+__device__ __forceinline__ SearchP search_params(const UnbArgs& A) {
+  return SearchP{A.nodes, A.obb, A.ltri, A.rec, A.pad, A.eD_abs, A.eD_rel, A.max_visits};
+}
+// m0: the lane's starting minimum (INFINITY, or a bound it must beat); keep_t / keep_d: its band
+// slots in shared memory (stride S), cleared by the caller.
+template <int S>
+__device__ __noinline__ SearchOut fp32_search(const SearchP A, int* stack, int lane, int rep, float3 p32, bool active,
+                                              float m0, int* keep_t, float* keep_d) {
+  LaneBest L;
+  L.m = m0;
+  L.overflow = false;
+  L.t = keep_t;
+  L.d = keep_d;
+  double m64 = kBig;
+  d3 proj = {0.0, 0.0, 0.0};
+  const d3 p = {0.0, 0.0, 0.0};  // the FP32 pass takes no FP64 step
+  int64_t fp64 = 0, visits = 0;
+  const bool ok = warp_search<false, S>(A, stack, lane, rep, p, p32, active, INFINITY, L, m64, proj, fp64, visits);
+  return SearchOut{L.m, L.overflow, ok, visits};
 }
 
 // FP64 steps over the kept triangles inside the final band, in ascending triangle index (so exact

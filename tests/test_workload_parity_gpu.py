@@ -69,12 +69,20 @@ def _ref_rule(ctx, X, IEN, g, n_uniform, n_near, seed):
 
 def _unbounded_and_learned(ctx, X, IEN, g, clamped, n_uniform, n_near, seed):
     ctx.set_mesh(X, IEN)
+    # each search twice, the faster time kept (a shared GPU can stall one call)
     plain, _ = ctx.distances(g["origin"], g["h"], g["N"], 2)
     ms_plain = ctx.stats()["ms_distance"]
+    plain2, _ = ctx.distances(g["origin"], g["h"], g["N"], 2)
+    ms_plain = min(ms_plain, ctx.stats()["ms_distance"])
+    assert np.array_equal(plain, plain2)
     ctx.train_radius(**TRAIN)
     ms_train = ctx.stats()["ms_train"]
     learned, _ = ctx.distances(g["origin"], g["h"], g["N"], 3)
+    ms_learned = ctx.stats()["ms_distance"]
+    learned2, _ = ctx.distances(g["origin"], g["h"], g["N"], 3)
     st = ctx.stats()
+    ms_learned = min(ms_learned, st["ms_distance"])
+    assert np.array_equal(learned, learned2)
     assert np.array_equal(plain, learned), "learned-radius search differs from the plain search"
     assert st["certified_nodes"] + st["unbounded_fallbacks"] == g["ngp"]
     assert np.all(np.minimum(plain, g["h"]) <= clamped)  # the clamped modes never go below the true minimum
@@ -84,7 +92,9 @@ def _unbounded_and_learned(ctx, X, IEN, g, clamped, n_uniform, n_near, seed):
                                       rng.choice(near, size=min(n_near, near.size), replace=False)])).astype(np.int64)
     dr, _, _ = oracle.distances(X, IEN, g["origin"], g["h"], g["N"], mode=2, nodes=nodes)
     _exact(learned[nodes], dr, X)
-    return ms_plain, st["ms_distance"], ms_train, st["certified_nodes"] / g["ngp"]
+    print(f"  learned search: {st['unbounded_fallbacks']} fallback nodes, "
+          f"{st['bvh_visits'] / g['ngp']:.2f} LBVH visits and {st['fp64_evals'] / g['ngp']:.2f} FP64 steps per node")
+    return ms_plain, ms_learned, ms_train, st["certified_nodes"] / g["ngp"]
 
 
 def test_blobs256_reference_rule_near_surface(gpu_ctx, blobs256):
