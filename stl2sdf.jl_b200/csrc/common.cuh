@@ -246,6 +246,7 @@ struct DistPlan {
   alignas(16) unsigned char knn_args[448];  // the fallback kernel's arguments (when knn)
   GridP g;
   int64_t ntiles = 0;
+  int64_t nonempty = -1;  // tiles with candidates (they come first in the fold's order); -1: unknown
   int threads = 0;
   bool knn = false;                         // the fallback runs after the fold
   uint8_t* band = nullptr;                  // nodes within h of a triangle (NULL: every empty node)

@@ -70,7 +70,7 @@ template <bool kFill>
 __global__ void k_tile_pairs(const double4* __restrict__ cent, const TriRec64* __restrict__ rec, int64_t nel,
                              GridP g, int mode, double R, int32_t* __restrict__ tri_cnt,
                              const int32_t* __restrict__ tri_off, int32_t* __restrict__ tile_cnt,
-                             uint32_t* __restrict__ keys, int32_t* __restrict__ vals) {
+                             uint32_t* __restrict__ keys, int32_t* __restrict__ vals, int32_t* __restrict__ nonempty) {
   for (int64_t el = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; el < nel; el += (int64_t)gridDim.x * blockDim.x) {
     double lo[3], hi[3];
     if (mode == SDFGPU_MODE_REF_RULE) {
@@ -115,7 +115,7 @@ __global__ void k_tile_pairs(const double4* __restrict__ cent, const TriRec64* _
               keys[base + count] = tile;
               vals[base + count] = (int32_t)el;
             } else {
-              atomicAdd(&tile_cnt[tile], 1);
+              if (atomicAdd(&tile_cnt[tile], 1) == 0) atomicAdd(nonempty, 1);  // the tile's first pair
             }
             ++count;
           }
@@ -351,6 +351,27 @@ __global__ void __launch_bounds__(256) k_tile_fold_multi(const FoldArgs* __restr
 }
 
 // Sort keys of the tile order: list length saturated to 16 bits, and the tile index.
+// The nodes of tiles without candidates: a node with an empty candidate set clamps to h
+// (dfOnTriangularMesh.jl:202-206; the 3-nearest-vertex fallback, when the mesh needs it, runs after
+// and finds these nodes by their status 0).  One coalesced pass over the nodes instead of a fold
+// CTA per empty tile; it writes exactly what fold_tile writes for such a tile.
+__global__ void k_fill_empty(GridP g, const int32_t* __restrict__ tile_cnt, double* __restrict__ dist,
+                             double* __restrict__ xp, uint8_t* __restrict__ status) {
+  for (int64_t lin = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; lin < g.ngp; lin += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i, j, k;
+    node_ijk(g, lin, i, j, k);
+    const int64_t tile = (k / g.t[2] * g.nt[1] + j / g.t[1]) * g.nt[0] + i / g.t[0];
+    if (tile_cnt[tile] != 0) continue;
+    dist[lin] = g.h;
+    status[lin] = 0;
+    if (xp) {
+      xp[3 * lin] = 0.0;
+      xp[3 * lin + 1] = 0.0;
+      xp[3 * lin + 2] = 0.0;
+    }
+  }
+}
+
 __global__ void k_tile_keys(const int32_t* __restrict__ cnt, int64_t n, uint16_t* __restrict__ key,
                             int32_t* __restrict__ idx) {
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
@@ -718,12 +739,16 @@ int dist_prepare(sdfgpu_ctx* ctx, const GridP& g, int mode, double* d_dist, doub
   SDF_TRY(scratch_t(ctx, "status", (size_t)g.ngp, &status));
   SDF_CUDA(ctx, cudaMemsetAsync(tile_cnt, 0, sizeof(int32_t) * (g.ntiles + 1), st));
   SDF_CUDA(ctx, cudaMemsetAsync(tri_cnt + nel, 0, sizeof(int32_t), st));
+  int32_t* nonempty;
+  SDF_TRY(scratch_t(ctx, "tile_nonempty", 1, &nonempty));
+  SDF_CUDA(ctx, cudaMemsetAsync(nonempty, 0, sizeof(int32_t), st));
   k_tile_pairs<false><<<grid_for(nel, 128), 128, 0, st>>>(cent, rec, nel, g, mode, R, tri_cnt, nullptr, tile_cnt,
-                                                          nullptr, nullptr);
+                                                          nullptr, nullptr, nonempty);
   SDF_KERNEL(ctx);
   SDF_TRY(cub_scan_i32(ctx, tri_cnt, tri_off, nel + 1));
-  int32_t total = 0;
+  int32_t total = 0, n_nonempty = 0;
   SDF_CUDA(ctx, cudaMemcpyAsync(&total, tri_off + nel, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  SDF_CUDA(ctx, cudaMemcpyAsync(&n_nonempty, nonempty, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   SDF_CUDA(ctx, cudaStreamSynchronize(st));
   if (total < 0) return fail(ctx, SDFGPU_ERR_CAPACITY, "more than 2^31 (tile, triangle) pairs; use a coarser grid");
   ctx->h_counters[C_TILE_PAIRS] = total;
@@ -734,7 +759,7 @@ int dist_prepare(sdfgpu_ctx* ctx, const GridP& g, int mode, double* d_dist, doub
   SDF_TRY(scratch_t(ctx, "pair_vals2", P, &vals2));
   if (total > 0) {
     k_tile_pairs<true><<<grid_for(nel, 128), 128, 0, st>>>(cent, rec, nel, g, mode, R, nullptr, tri_off, nullptr,
-                                                           keys, vals);
+                                                           keys, vals, nullptr);
     SDF_KERNEL(ctx);
     const int bits = ceil_log2((uint64_t)g.ntiles + 1);
     size_t tmp_bytes = 0;
@@ -789,6 +814,7 @@ int dist_prepare(sdfgpu_ctx* ctx, const GridP& g, int mode, double* d_dist, doub
   std::memcpy(Pl.fold, &A, sizeof(A));
   Pl.g = g;
   Pl.ntiles = g.ntiles;
+  Pl.nonempty = n_nonempty;
   Pl.threads = g.t[0] * g.t[1] * g.t[2];
   Pl.knn = false;
   if (mode == SDFGPU_MODE_REF_RULE) {
@@ -835,8 +861,17 @@ int dist_fold(sdfgpu_ctx* ctx, const DistPlan& Pl) {
   const size_t smem = sizeof(WarpStage) * (size_t)(Pl.threads / 32);
   if (smem > 48 * 1024)  // tiles of more than 5 warps stage more than the default 48 KB
     SDF_CUDA(ctx, cudaFuncSetAttribute(k_tile_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_tile_fold<<<(unsigned)Pl.ntiles, Pl.threads, smem, ctx->stream>>>(A);
-  SDF_KERNEL(ctx);
+  // the tiles with candidates come first in the fold's order (longest list first); the rest are
+  // written by one pass over the nodes
+  const int64_t nfold = Pl.nonempty >= 0 ? Pl.nonempty : Pl.ntiles;
+  if (nfold < Pl.ntiles) {
+    k_fill_empty<<<grid_for(Pl.g.ngp, 256), 256, 0, ctx->stream>>>(Pl.g, A.tile_cnt, A.dist, A.xp, A.status);
+    SDF_KERNEL(ctx);
+  }
+  if (nfold > 0) {
+    k_tile_fold<<<(unsigned)nfold, Pl.threads, smem, ctx->stream>>>(A);
+    SDF_KERNEL(ctx);
+  }
   return 0;
 }
 
