@@ -294,6 +294,10 @@ def run_batch(args, rank, world, local):
     ctx.sdf_batch(mine, out=outs, streams=args.streams, autotune=True, mode=_nat.MODE_LEARNED)  # tuning, buffers
     lrn, _ = timed(1, streams=args.streams, autotune=True, mode=_nat.MODE_LEARNED)
     lst = ctx.stats()
+    # ... and with every mesh's search in one persistent launch (two with the radius) in a CUDA graph
+    ctx.sdf_batch(mine, out=outs, streams=args.streams, autotune=True, mode=_nat.MODE_LEARNED, persistent=True)
+    lrp, _ = timed(1, streams=args.streams, autotune=True, mode=_nat.MODE_LEARNED, persistent=True)
+    lpst = ctx.stats()
     total = sum(ngps)
     value = total * args.steps / dt
     line = {
@@ -318,6 +322,13 @@ def run_batch(args, rank, world, local):
                                 "fallback_rate": lst["unbounded_fallbacks"] / max(1, lst["ngp"]),
                                 "note": "SDFGPU_MODE_LEARNED: unbounded distances, one radius network trained per "
                                         "mesh inside the call (training time included)"},
+        "learned_radius_persistent_form": {"value": total / lrp, "s": lrp, "train_ms_summed": lpst["ms_train"],
+                                           "search_ms": lpst["ms_distance"],
+                                           "certified_fraction": lpst["certified_nodes"] / max(1, lpst["ngp"]),
+                                           "fallback_rate": lpst["unbounded_fallbacks"] / max(1, lpst["ngp"]),
+                                           "note": "SDFGPU_MODE_LEARNED, sdfgpu_sdf_batch_ex(persistent=1): networks "
+                                                   "trained while the items are prepared, every mesh's search in one "
+                                                   "persistent launch inside a CUDA graph"},
         "first_call_s": t_tune,
         "stages_ms_summed": {k: st[k] for k in ("ms_mesh", "ms_tiles", "ms_fold", "ms_rows", "ms_parity", "ms_vote")},
         "counters_summed": {k: st[k] for k in ("tile_pairs", "fp64_evals", "row_hits", "undecided_nodes", "extra_rays",

@@ -235,19 +235,23 @@ int sdfgpu_sdf_batch(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count, i
                      int32_t max_rays, double confidence_threshold, int32_t use_winding_fallback, int32_t streams,
                      int32_t autotune);
 
-/* sdfgpu_sdf_batch with the choice of how the reference-rule and h-bounded modes run (results are
- * the same either way).  persistent = 0: each item runs the whole per-mesh pipeline on one of the
- * worker streams (sdfgpu_sdf_batch does this).  persistent = 1: the workers first prepare every
- * item (mesh, LBVH, tile lists, sign stage) in item-private buffers; then one CUDA graph runs the
- * folds of all items in a single persistent kernel launch (CTAs striding over the batch's (item,
- * tile) work list, every item with its own tile) followed by each item's nearest-vertex fallback
- * and combine on the worker streams side by side; then the fields are copied out.  Items go to the
+/* sdfgpu_sdf_batch with the choice of how the batch runs (results are the same either way).
+ * persistent = 0: each item runs the whole per-mesh pipeline on one of the worker streams
+ * (sdfgpu_sdf_batch does this).  persistent = 1: the workers first prepare every item (mesh, LBVH,
+ * the sign stage, and the distance stage up to its last kernel: the tile lists of the reference-rule
+ * and h-bounded modes; the search arguments and, in the learned mode, the radius network and the
+ * radius of every warp brick of the unbounded and learned modes) in item-private buffers; then one
+ * CUDA graph runs the distance kernels of all items in a single persistent launch -- the folds,
+ * CTAs striding over the batch's (item, tile) work list, every item with its own tile; or the
+ * searches, warps taking (item, brick) work items from one queue, with a second launch for the
+ * bricks the learned radius did not certify -- followed by each item's nearest-vertex fallback and
+ * combine on the worker streams side by side; then the fields are copied out.  Items go to the
  * workers by a fixed longest-processing-time assignment, so repeated batches reuse their buffers.
- * Unbounded and learned-radius batches always run per item.  With mode = SDFGPU_MODE_LEARNED
- * every mesh gets its own radius network, trained right after its LBVH with the options of the last
- * sdfgpu_train_radius on ctx (defaults: 200 steps, batch 2048, learning rate 5e-3, seed 0) on a
- * coarse grid of min(32, K / 2) nodes on its longest axis (at least 16), K the nodes on the longest
- * axis of the mesh's own grid; results equal SDFGPU_MODE_UNBOUNDED. */
+ * With mode = SDFGPU_MODE_LEARNED every mesh gets its own radius network, trained right after its
+ * LBVH with the options of the last sdfgpu_train_radius on ctx (defaults: 200 steps, batch 2048,
+ * learning rate 5e-3, seed 0) and ctx's search margin (sdfgpu_set_radius_margin) on a coarse grid of
+ * min(32, K / 2) nodes on its longest axis (at least 16), K the nodes on the longest axis of the
+ * mesh's own grid; results equal SDFGPU_MODE_UNBOUNDED. */
 int sdfgpu_sdf_batch_ex(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count, int32_t mode, int32_t min_rays,
                         int32_t max_rays, double confidence_threshold, int32_t use_winding_fallback, int32_t streams,
                         int32_t autotune, int32_t persistent);

@@ -15,10 +15,13 @@
 //      item), followed by every item's 3-nearest-vertex fallback and combine -- the whole sequence
 //      captured in one CUDA graph and launched once;
 //   3. the fields are copied to the callers' buffers.
-// Unbounded batches keep the per-item pipeline (their search has no tile lists).  Learned-radius
-// batches (SDFGPU_MODE_LEARNED) too: every worker trains a network for each of its meshes (on a
-// coarse grid of at most half the mesh grid's nodes per axis) right after the mesh's LBVH, then
-// runs the learned search of that mesh.
+// Unbounded and learned-radius batches (SDFGPU_MODE_UNBOUNDED / _LEARNED) take the same phases:
+// phase 1 stops the distance stage at the search's arguments (and, learned, trains each mesh's
+// radius network on a coarse grid of at most half the mesh grid's nodes per axis and predicts the
+// radius of every warp brick); phase 2's persistent launch is the multi-mesh search
+// (k_unbounded_multi: warps take (item, brick) work items from one queue; with the radius, a second
+// launch reruns the bricks the first did not certify).  In the per-item form a worker trains and
+// searches each mesh in turn.
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -172,6 +175,20 @@ int pick_tile(BatchJob& J, sdfgpu_ctx* w, const sdfgpu_batch_item& it) {
   return 0;
 }
 
+// An item's radius network (SDFGPU_MODE_LEARNED), on a coarse grid of its own: at most half the
+// nodes of the item's grid per axis, the batch context's other training options and search margin.
+int train_item(BatchJob& J, sdfgpu_ctx* w, const sdfgpu_batch_item& it, sdfgpu_stats& ms) {
+  const int64_t K = std::max(it.N[0], std::max(it.N[1], it.N[2])) + 1;
+  const int coarse = (int)std::max<int64_t>(16, std::min<int64_t>(J.train.train_coarse, K / 2));
+  const int rc = sdfgpu_train_radius(w, coarse, J.train.train_steps, J.train.train_batch, J.train.train_lr,
+                                     J.train.train_seed, nullptr);
+  ms.ms_train = w->stats.ms_train;
+  ms.train_launches = w->stats.train_launches;
+  w->radius.alpha = J.train.alpha;  // the batch context's search margin
+  w->radius.beta = J.train.beta;
+  return rc;
+}
+
 void worker_main(BatchJob& J, sdfgpu_ctx* w) {
   const int64_t n = (int64_t)J.order.size();
   w->ns.clear();
@@ -183,14 +200,7 @@ void worker_main(BatchJob& J, sdfgpu_ctx* w) {
     sdfgpu_batch_item& it = J.items[i];
     int rc = sdfgpu_set_mesh(w, it.X, it.nnp, it.IEN, it.nel);
     sdfgpu_stats ms = w->stats;
-    if (rc == 0 && J.mode == SDFGPU_MODE_LEARNED) {  // this mesh's network, on a coarse grid of its own
-      const int64_t K = std::max(it.N[0], std::max(it.N[1], it.N[2])) + 1;
-      const int coarse = (int)std::max<int64_t>(16, std::min<int64_t>(J.train.train_coarse, K / 2));
-      rc = sdfgpu_train_radius(w, coarse, J.train.train_steps, J.train.train_batch, J.train.train_lr,
-                               J.train.train_seed, nullptr);
-      ms.ms_train = w->stats.ms_train;
-      ms.train_launches = w->stats.train_launches;
-    }
+    if (rc == 0 && J.mode == SDFGPU_MODE_LEARNED) rc = train_item(J, w, it, ms);
     if (rc == 0 && J.autotune) rc = pick_tile(J, w, it);
     if (rc == 0)
       rc = sdfgpu_sdf(w, it.origin, it.h, it.N, J.mode, J.min_rays, J.max_rays, J.conf, J.use_winding, it.sdf, it.dist,
@@ -232,6 +242,7 @@ void worker_prepare(BatchJob& J, sdfgpu_ctx* w, const std::vector<int64_t>& mine
     w->ns = "s" + std::to_string(slot++) + ":";
     int rc = sdfgpu_set_mesh(w, it.X, it.nnp, it.IEN, it.nel);
     sdfgpu_stats ms = w->stats;
+    if (rc == 0 && J.mode == SDFGPU_MODE_LEARNED) rc = train_item(J, w, it, ms);
     if (rc == 0 && J.autotune) rc = pick_tile(J, w, it);
     GridP g;
     if (rc == 0) rc = make_grid(w, it.origin, it.h, it.N, g);
@@ -272,25 +283,45 @@ int run_persistent(sdfgpu_ctx* ctx, BatchJob& J, std::vector<Prepared>& prep, in
     SDF_CUDA(ctx, cudaStreamSynchronize(w->bvh_stream));
   }
   const int64_t count = (int64_t)prep.size();
-  const size_t sz = fold_args_size();
+  // unbounded / learned items: one search over every (item, brick) work item (plan.unb); the others
+  // one fold over every (item, tile)
+  const bool unb = prep[0].plan.unbounded;
+  bool radius = unb;
+  for (const Prepared& P : prep) radius = radius && P.plan.unb_radius;
+  const size_t sz = unb ? unb_args_size() : fold_args_size();
   std::vector<unsigned char> args(sz * (size_t)count);
-  std::vector<int64_t> off((size_t)count);
+  std::vector<int64_t> off((size_t)count + 1);
   int64_t total = 0;
   for (int64_t i = 0; i < count; ++i) {
-    plan_set_counters(prep[i].plan, ctx->d_counters);
-    std::memcpy(args.data() + sz * (size_t)i, prep[i].plan.fold, sz);
     off[(size_t)i] = total;
-    total += prep[i].plan.ntiles;
+    total += unb ? prep[i].plan.nbricks : prep[i].plan.ntiles;
+  }
+  off[(size_t)count] = total;
+  int64_t* redo = nullptr;
+  unsigned long long* heads = nullptr;
+  if (unb) {
+    SDF_TRY(scratch_t(ctx, "batch_redo", (size_t)total, &redo));
+    SDF_TRY(scratch_t(ctx, "batch_heads", 3, &heads));
+  }
+  for (int64_t i = 0; i < count; ++i) {
+    if (unb) {
+      plan_set_redo(prep[i].plan, redo, heads + 2, off[(size_t)i]);
+      std::memcpy(args.data() + sz * (size_t)i, prep[i].plan.unb, sz);
+    } else {
+      plan_set_counters(prep[i].plan, ctx->d_counters);
+      std::memcpy(args.data() + sz * (size_t)i, prep[i].plan.fold, sz);
+    }
   }
   void* d_args;
   int64_t* d_off;
   SDF_TRY(scratch(ctx, "batch_args", args.size(), &d_args));
-  SDF_TRY(scratch_t(ctx, "batch_off", (size_t)count, &d_off));
+  SDF_TRY(scratch_t(ctx, "batch_off", (size_t)count + 1, &d_off));
   SDF_TRY(reset_counters(ctx));
   SDF_CUDA(ctx, cudaMemcpyAsync(d_args, args.data(), args.size(), cudaMemcpyHostToDevice, st));
-  SDF_CUDA(ctx, cudaMemcpyAsync(d_off, off.data(), sizeof(int64_t) * count, cudaMemcpyHostToDevice, st));
+  SDF_CUDA(ctx, cudaMemcpyAsync(d_off, off.data(), sizeof(int64_t) * (count + 1), cudaMemcpyHostToDevice, st));
   int64_t grid = 1;
-  SDF_TRY(dist_fold_multi_grid(ctx, threads, total, &grid));
+  if (unb) SDF_TRY(unb_multi_grid(ctx, total, &grid));
+  else SDF_TRY(dist_fold_multi_grid(ctx, threads, total, &grid));
   SDF_CUDA(ctx, cudaStreamSynchronize(st));  // the argument arrays are in place before the capture
 
   // the items' fallbacks and combines after the fold, on the (idle) worker streams side by side
@@ -304,7 +335,8 @@ int run_persistent(sdfgpu_ctx* ctx, BatchJob& J, std::vector<Prepared>& prep, in
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   SDF_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-  int rc = dist_fold_multi(ctx, d_args, d_off, (int)count, total, threads, grid, st);
+  int rc = unb ? unb_multi(ctx, d_args, d_off, (int)count, radius, redo, heads, grid, st)
+               : dist_fold_multi(ctx, d_args, d_off, (int)count, total, threads, grid, st);
   if (rc == 0 && cudaEventRecord(evs[(size_t)nw], st) != cudaSuccess) rc = fail(ctx, SDFGPU_ERR_CUDA, "batch fork");
   for (int k = 0; k < nw && rc == 0; ++k)
     if (cudaStreamWaitEvent(ctx->workers[k]->stream, evs[(size_t)nw], 0) != cudaSuccess)
@@ -354,6 +386,9 @@ int run_persistent(sdfgpu_ctx* ctx, BatchJob& J, std::vector<Prepared>& prep, in
   J.stats.fp64_evals += c[C_FP64];
   J.stats.candidate_nodes += c[C_CAND_NODES];
   J.stats.knn_fallback_nodes += c[C_KNN];
+  J.stats.certified_nodes += c[C_CERTIFIED];
+  J.stats.unbounded_fallbacks += c[C_UNB_FALLBACK];
+  J.stats.bvh_visits += c[C_VISITS];
   J.stats.ms_fold += ms;
   J.stats.ms_distance += ms;
   J.stats.launches += 1 + count;
@@ -438,7 +473,7 @@ int sdfgpu_sdf_batch_ex(sdfgpu_ctx* ctx, sdfgpu_batch_item* items, int64_t count
       }
   std::vector<std::thread> threads;
   threads.reserve(nw);
-  if (mode == SDFGPU_MODE_UNBOUNDED || mode == SDFGPU_MODE_LEARNED || !persistent) {  // per-item pipelines
+  if (!persistent) {  // per-item pipelines
     for (int k = 0; k < nw; ++k) threads.emplace_back(worker_main, std::ref(J), ctx->workers[k]);
     for (auto& t : threads) t.join();
     ctx->stats = J.stats;

@@ -267,7 +267,7 @@ int run_all(sdfgpu_ctx* ctx, const GridP& g, bool want_dist, bool want_sign, int
     }
     if (want_dist) {
       if (defer)  // a batch runs the fold later, together with other meshes'
-        SDF_TRY(dist_prepare(ctx, g, mode, d_dist, d_xp, *defer));
+        SDF_TRY(dist_prepare(ctx, g, mode, d_dist, d_xp, *defer, learned));
       else
         SDF_TRY(run_distances(ctx, g, mode, learned, d_dist, d_xp));
     }

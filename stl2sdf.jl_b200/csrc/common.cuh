@@ -244,6 +244,10 @@ int run_nearest_points(sdfgpu_ctx* ctx, const GridP& g, double* d_dist);
 struct DistPlan {
   alignas(16) unsigned char fold[448];      // the fold kernel's arguments
   alignas(16) unsigned char knn_args[448];  // the fallback kernel's arguments (when knn)
+  alignas(16) unsigned char unb[512];       // unbounded / learned: the search's arguments (UnbArgs)
+  bool unbounded = false;                   // the plan is an unbounded search (unb), not a fold
+  bool unb_radius = false;                  // ... started from the learned radius
+  int64_t nbricks = 0;                      // ... over this many warp bricks
   GridP g;
   int64_t ntiles = 0;
   int64_t nonempty = -1;  // tiles with candidates (they come first in the fold's order); -1: unknown
@@ -255,7 +259,8 @@ struct DistPlan {
   int64_t nel = 0;
   double hb = 0.0;
 };
-int dist_prepare(sdfgpu_ctx* ctx, const GridP& g, int mode, double* d_dist, double* d_xp, DistPlan& P);
+int dist_prepare(sdfgpu_ctx* ctx, const GridP& g, int mode, double* d_dist, double* d_xp, DistPlan& P,
+                 int use_learned = 0);
 int dist_fold(sdfgpu_ctx* ctx, const DistPlan& P);
 int dist_knn(sdfgpu_ctx* ctx, const DistPlan& P, cudaStream_t st, bool wait_bvh);
 int dist_fold_multi_grid(sdfgpu_ctx* ctx, int threads, int64_t total, int64_t* grid);
@@ -263,6 +268,14 @@ int dist_fold_multi(sdfgpu_ctx* ctx, const void* d_args, const int64_t* d_off, i
                     int64_t grid, cudaStream_t st);
 size_t fold_args_size();
 void plan_set_counters(DistPlan& P, int64_t* counters);
+// The unbounded / learned counterparts for a batch (distance.cu): dist_prepare fills plan.unb when
+// the mode is SDFGPU_MODE_UNBOUNDED; unb_multi runs the searches of many such plans in one
+// persistent launch (two with the learned radius).
+size_t unb_args_size();
+void plan_set_redo(DistPlan& P, int64_t* redo, unsigned long long* redo_n, int64_t base);
+int unb_multi_grid(sdfgpu_ctx* ctx, int64_t total, int64_t* grid);
+int unb_multi(sdfgpu_ctx* ctx, const void* d_items, const int64_t* d_off, int count, bool radius, int64_t* redo,
+              unsigned long long* heads, int64_t grid, cudaStream_t st);
 int launch_combine(sdfgpu_ctx* ctx, int64_t ngp, const double* d_dist, const double* d_sign, double* d_sdf,
                    cudaStream_t st);
 // The sign stage in two parts on ctx->sign_stream: sign_begin enqueues the axis-row counting and

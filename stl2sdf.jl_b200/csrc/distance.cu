@@ -519,7 +519,9 @@ __global__ void k_knn_fallback(KnnArgs A) {
 // that starts each lane's minimum at its radius r; a brick with a lane that the pass does not
 // certify is appended to A.redo and left unwritten.  kUnbListed: the plain search over the bricks
 // listed in A.bricks (the learned mode's second launch).
-constexpr int kUnbPlain = 0, kUnbRadius = 1, kUnbListed = 2;
+
+
+
 template <int kMode>
 __global__ void __launch_bounds__(kUnbThreads, 4) k_unbounded(UnbArgs A) {
   constexpr bool kRadius = kMode == kUnbRadius, kListed = kMode == kUnbListed;
@@ -540,79 +542,7 @@ __global__ void __launch_bounds__(kUnbThreads, 4) k_unbounded(UnbArgs A) {
   const int64_t total = kListed ? (int64_t)*A.bricks_n : A.nbricks;
   for (int64_t q = next_brick(A, lane); q < total; q = next_brick(A, lane)) {
     const int64_t brick = kListed ? A.bricks[q] : q;
-    const int64_t bx = brick % A.nb[0], by = (brick / A.nb[0]) % A.nb[1], bz = brick / (A.nb[0] * A.nb[1]);
-    const int64_t i = bx * A.b[0] + lx, j = by * A.b[1] + ly, k = bz * A.b[2] + lz;
-    const bool valid = i <= g.N[0] && j <= g.N[1] && k <= g.N[2];
-    // lanes past the grid edge stand on the nearest grid node (they only order the traversal)
-    const d3 p = gnode(g, min(i, g.N[0]), min(j, g.N[1]), min(k, g.N[2]));
-    const float3 p32 = local32(g, p);
-    const int64_t lin = i + g.n[0] * (j + g.n[1] * k);
-    LaneBest L;
-    L.m = INFINITY;
-    L.overflow = false;
-    L.t = s_keep_t + threadIdx.x;
-    L.d = s_keep_d + threadIdx.x;
-#pragma unroll
-    for (int q = 0; q < kKeep; ++q) {
-      L.t[q * kUnbThreads] = -1;
-      L.d[q * kUnbThreads] = INFINITY;
-    }
-    double m64 = kBig;
-    d3 proj = {0.0, 0.0, 0.0};
-    // kRadius: the lane's FP32 minimum starts at r -- the brick's radius plus the node's distance
-    // from the brick centre where it was predicted -- as if a triangle lay there, and the pass is the
-    // plain search from that state.  A triangle with FP32 distance below r is never pruned (its box
-    // bound is below r, and every bound of the lane stays >= its minimum), so a lane that ends below
-    // r holds the true FP32 minimum and its band, exactly as the unbounded search would: it is
-    // certified.  A brick with a lane left at r goes to the plain search of the listed bricks.
-    if (kRadius && valid) {
-      const d3 c = brick_center(g, A.b, bx, by, bz);
-      const double dx = p.x - c.x, dy = p.y - c.y, dz = p.z - c.z;
-      L.m = (float)((double)A.radius[brick] + sqrt(dx * dx + dy * dy + dz * dz));
-      s_r[threadIdx.x] = L.m;
-    }
-    // the FP32 pass: inlined in the plain kernels, out of line in the radius-started one (each the
-    // faster form for its kernel: 78.9 against 80.6 ms plain, 80.8 against 84.1 ms radius-started
-    // on the 14.3M-node blob grid)
-    bool ok;
-    if constexpr (kRadius) {
-      const SearchOut so = fp32_search<kUnbThreads>(search_params(A), stack, lane, rep, p32, valid, L.m, L.t, L.d);
-      L.m = so.m;
-      L.overflow = so.overflow;
-      visits += so.visits;
-      ok = so.ok;
-    } else {
-      ok = warp_search<false, kUnbThreads>(A, stack, lane, rep, p, p32, valid, INFINITY, L, m64, proj, fp64, visits);
-    }
-    if (kRadius && ok) {
-      const bool certified = valid && L.m < s_r[threadIdx.x];
-      const unsigned nc = __popc(__ballot_sync(0xffffffffu, valid && certified));
-      const unsigned nf = __popc(__ballot_sync(0xffffffffu, valid && !certified));
-      if (lane == 0) {
-        s_cf[w][0] += nc;
-        s_cf[w][1] += nf;
-      }
-      if (nf) {  // the whole brick again, unbounded
-        if (lane == 0) {  // lane 0 stands on the brick's first node (always inside the grid)
-          const int64_t i0 = lin % g.n[0], j0 = (lin / g.n[0]) % g.n[1], k0 = lin / (g.n[0] * g.n[1]);
-          A.redo[atomicAdd(A.redo_n, 1ULL)] = i0 / A.b[0] + A.nb[0] * (j0 / A.b[1] + A.nb[1] * (k0 / A.b[2]));
-        }
-        continue;
-      }
-    }
-    const bool over = valid && L.overflow;
-    if (ok && __any_sync(0xffffffffu, over))
-      ok = warp_search<true, kUnbThreads>(A, stack, lane, rep, p, p32, over, band_of(A, L.m), L, m64, proj, fp64, visits);
-    if (valid && !over) lane_resolve<kUnbThreads>(A, L, p, m64, proj, fp64);
-    if (!ok && lane == 0) ++errs;
-    if (valid) {
-      A.dist[lin] = m64;
-      if (A.xp) {
-        A.xp[3 * lin] = proj.x;
-        A.xp[3 * lin + 1] = proj.y;
-        A.xp[3 * lin + 2] = proj.z;
-      }
-    }
+#include "unb_brick.inc"
   }
   for (int off = 16; off > 0; off >>= 1) fp64 += __shfl_down_sync(0xffffffffu, fp64, off);
   if (lane == 0) {
@@ -624,6 +554,7 @@ __global__ void __launch_bounds__(kUnbThreads, 4) k_unbounded(UnbArgs A) {
   }
 }
 
+
 int ceil_log2(uint64_t v) {
   int b = 0;
   while ((1ULL << b) < v) ++b;
@@ -632,47 +563,49 @@ int ceil_log2(uint64_t v) {
 
 }  // namespace
 
+namespace {
+
+// The unbounded search's arguments for grid g on the current mesh (FP32 error model as in
+// run_distances), with the learned radius of every brick when use_learned and the network's bound
+// is on; the context stream waits for the LBVH and its oriented boxes.
+int unb_setup(sdfgpu_ctx* ctx, const GridP& g, int use_learned, double* d_dist, double* d_xp, UnbArgs& A) {
+  // FP32 error model: coordinates in the mesh-local frame are within E, so each FP32 coordinate
+  // carries at most 2^-24 E; the distance band (4e-6 E + 4e-6 d) keeps a >= 5x margin over the
+  // worst accumulation, the box margin kUnbPadRel E a >= 8x one.
+  const float E = (float)g.E;
+  SDF_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_obb, 0));  // the search walks the LBVH and its oriented boxes
+  A = UnbArgs{g, buf<BNode>(ctx, "nodes"), buf<LeafTri>(ctx, "ltri"), buf<TriRec64>(ctx, "rec"), kUnbPadRel * E,
+             4.0e-6f * E, 4.0e-6f, 2 * ctx->mesh.nel + 64, nullptr, d_dist, d_xp, ctx->d_counters};
+  A.obb = buf<OBox>(ctx, "obb");
+  A.nbricks = 1;
+  for (int a = 0; a < 3; ++a) {
+    A.b[a] = ctx->brick[a];
+    A.nb[a] = cdiv(g.n[a], A.b[a]);
+    A.nbricks *= A.nb[a];
+  }
+  if (use_learned) {
+    // the network's radius at each brick centre c, rc = (dhat (1 + alpha) + beta * coarse spacing
+    // / s) s (a margin for the network's error and for the interpolation between its training
+    // nodes); a node p of the brick searches within rc + |p - c| (k_unbounded).  alpha = +inf:
+    // no radius, the same search without the network's bound.
+    const RadiusNorm& R = ctx->radius;
+    if (!std::isinf(R.alpha)) {
+      float* radius;
+      SDF_TRY(scratch_t(ctx, "radius", (size_t)A.nbricks, &radius));
+      SDF_TRY(run_radius(ctx, &g, nullptr, A.nbricks, R.alpha, (float)(R.beta * R.coarse_h / R.s), radius, A.b));
+      A.radius = radius;
+    }
+  }
+  return 0;
+}
+
+}  // namespace
+
 int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, double* d_dist, double* d_xp) {
   cudaStream_t st = ctx->stream;
-  const MeshDev& M = ctx->mesh;
-  const int64_t nel = M.nel;
-  TriRec64* rec = buf<TriRec64>(ctx, "rec");
-  double4* cent = buf<double4>(ctx, "cent64");
-  float4* v32 = buf<float4>(ctx, "v32");
-  float4* c32 = buf<float4>(ctx, "c32");
-  BNode* nodes = buf<BNode>(ctx, "nodes");
-  int32_t* leaf_prim = buf<int32_t>(ctx, "leaf_prim");
-  // FP32 error model: coordinates in the mesh-local frame are within E, so each FP32 coordinate
-  // carries at most 2^-24 E; the bounds below keep a >= 8x margin over the worst accumulation.
-  const float E = (float)g.E;
-  const float eD_abs = 4.0e-6f * E;
-  const float eD_rel = 4.0e-6f;
-  const float pad = 2.0e-6f * E;
-
   if (mode == SDFGPU_MODE_UNBOUNDED) {
-    SDF_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev_obb, 0));  // the search walks the LBVH and its oriented boxes
-    UnbArgs A{g, nodes, buf<LeafTri>(ctx, "ltri"), rec, kUnbPadRel * E, eD_abs, eD_rel, 2 * nel + 64, nullptr, d_dist,
-              d_xp, ctx->d_counters};
-    A.obb = buf<OBox>(ctx, "obb");
-    A.nbricks = 1;
-    for (int a = 0; a < 3; ++a) {
-      A.b[a] = ctx->brick[a];
-      A.nb[a] = cdiv(g.n[a], A.b[a]);
-      A.nbricks *= A.nb[a];
-    }
-    if (use_learned) {
-      // the network's radius at each brick centre c, rc = (dhat (1 + alpha) + beta * coarse spacing
-      // / s) s (a margin for the network's error and for the interpolation between its training
-      // nodes); a node p of the brick searches within rc + |p - c| (k_unbounded).  alpha = +inf:
-      // no radius, the same search without the network's bound.
-      const RadiusNorm& R = ctx->radius;
-      if (!std::isinf(R.alpha)) {
-        float* radius;
-        SDF_TRY(scratch_t(ctx, "radius", (size_t)A.nbricks, &radius));
-        SDF_TRY(run_radius(ctx, &g, nullptr, A.nbricks, R.alpha, (float)(R.beta * R.coarse_h / R.s), radius, A.b));
-        A.radius = radius;
-      }
-    }
+    UnbArgs A;
+    SDF_TRY(unb_setup(ctx, g, use_learned, d_dist, d_xp, A));
     SDF_MARK(ctx, T_TILES);
     // one resident wave of CTAs draining the brick queue: queue heads of the two launches and the
     // count of bricks handed from the bounded to the plain search, zeroed together
@@ -713,7 +646,24 @@ int run_distances(sdfgpu_ctx* ctx, const GridP& g, int mode, int use_learned, do
 
 // Tile lists of the reference rule (or the h-bounded exact mode) and the fold's arguments; when the
 // mesh needs the 3-nearest-vertex fallback, its incidence lists, band flags and arguments too.
-int dist_prepare(sdfgpu_ctx* ctx, const GridP& g, int mode, double* d_dist, double* d_xp, DistPlan& Pl) {
+// A batch item's unbounded (or learned) search, prepared for the multi-mesh launch: its arguments
+// and, in the learned mode, the radius of every brick, in the item's own buffers.
+int unb_prepare(sdfgpu_ctx* ctx, const GridP& g, int use_learned, double* d_dist, double* d_xp, DistPlan& Pl) {
+  UnbArgs A;
+  SDF_TRY(unb_setup(ctx, g, use_learned, d_dist, d_xp, A));
+  std::memcpy(Pl.unb, &A, sizeof(A));
+  Pl.g = g;
+  Pl.unbounded = true;
+  Pl.unb_radius = A.radius != nullptr;
+  Pl.nbricks = A.nbricks;
+  Pl.ntiles = 0;
+  Pl.knn = false;
+  return 0;
+}
+
+int dist_prepare(sdfgpu_ctx* ctx, const GridP& g, int mode, double* d_dist, double* d_xp, DistPlan& Pl,
+                 int use_learned) {
+  if (mode == SDFGPU_MODE_UNBOUNDED) return unb_prepare(ctx, g, use_learned, d_dist, d_xp, Pl);
   static_assert(sizeof(FoldArgs) <= sizeof(Pl.fold), "DistPlan::fold too small");
   static_assert(sizeof(KnnArgs) <= sizeof(Pl.knn_args), "DistPlan::knn_args too small");
   cudaStream_t st = ctx->stream;
@@ -919,6 +869,7 @@ int dist_fold_multi(sdfgpu_ctx* ctx, const void* d_args, const int64_t* d_off, i
 }
 
 size_t fold_args_size() { return sizeof(FoldArgs); }
+
 
 // Points a plan's kernels at another counter array (a batch sums its folds' counters in one place).
 void plan_set_counters(DistPlan& Pl, int64_t* counters) {

@@ -58,6 +58,7 @@ struct UnbArgs {
   const unsigned long long* bricks_n = nullptr;  // ... this many (read on the device)
   int64_t* redo = nullptr;                       // the radius-bounded search lists here the bricks ...
   unsigned long long* redo_n = nullptr;          // ... it did not certify (a counter zeroed per launch)
+  int64_t redo_base = 0;                         // added to the listed brick index (a batch's item offset)
 };
 
 // FP32 margin of every box test of the unbounded searches, as a multiple of the frame's scale E:
@@ -80,6 +81,18 @@ __device__ __forceinline__ float child_d2(const BNode& nd, const OBox& o, int si
   const int c = side ? nd.d.y : nd.d.x;
   if (c & kLeafBit) return d;
   return fmaxf(d, obox_d2(p, o));
+}
+
+// Instantiations of the grid searches (k_unbounded, distance.cu; k_unbounded_multi, search_multi.cu):
+// kUnbPlain every brick unbounded; kUnbRadius each lane started from its learned radius;
+// kUnbListed the plain search over listed bricks.
+constexpr int kUnbPlain = 0, kUnbRadius = 1, kUnbListed = 2;
+// Lane `lane`'s node (lx, ly, lz) in a warp brick of shape b, and the brick's central lane rep.
+__device__ __forceinline__ void brick_lane(const int32_t b[3], int lane, int& lx, int& ly, int& lz, int& rep) {
+  lx = lane % b[0];
+  ly = (lane / b[0]) % b[1];
+  lz = lane / (b[0] * b[1]);
+  rep = b[0] / 2 + b[0] * (b[1] / 2 + b[1] * (b[2] / 2));
 }
 
 // The warp's next brick from the launch's queue (bricks differ widely in cost, so a static split

@@ -158,19 +158,24 @@ def test_workload_batch_items_match_oracle(gpu_ctx):
 
 
 def test_learned_batch_equals_unbounded_and_oracle(gpu_ctx, small_batch):
-    """SDFGPU_MODE_LEARNED over the uneven batch: every mesh trains its own radius network inside
-    the call; the fields equal the plain unbounded batch bit for bit, and sampled nodes of three
-    meshes equal the oracle's unbounded distance and its sign."""
+    """SDFGPU_MODE_LEARNED over the uneven batch, in both forms (per-item pipelines; prepared items
+    whose searches all run in one persistent launch, two with the radius, inside a CUDA graph): every
+    mesh trains its own radius network inside the call; the fields equal the plain unbounded batch
+    bit for bit, every node is certified or counted as a fallback, and sampled nodes of three meshes
+    equal the oracle's unbounded distance and its sign."""
     from stl2sdf import _native
 
     plain = gpu_ctx.sdf_batch(small_batch, mode=_native.MODE_UNBOUNDED, streams=4, autotune=True, want_parts=True)
-    learned = gpu_ctx.sdf_batch(small_batch, mode=_native.MODE_LEARNED, streams=4, autotune=True, want_parts=True)
-    st = gpu_ctx.stats()
-    assert st["certified_nodes"] + st["unbounded_fallbacks"] == st["ngp"]
-    assert st["train_launches"] > 0 and st["ms_train"] > 0
-    for a, b in zip(learned, plain):
-        for x, y in zip(a, b):
-            assert np.array_equal(x, y)
+    for persistent in (False, True):
+        learned = gpu_ctx.sdf_batch(small_batch, mode=_native.MODE_LEARNED, streams=4, autotune=True, want_parts=True,
+                                    persistent=persistent)
+        st = gpu_ctx.stats()
+        assert st["certified_nodes"] + st["unbounded_fallbacks"] == st["ngp"]
+        assert st["certified_nodes"] > 0.9 * st["ngp"]
+        assert st["train_launches"] > 0 and st["ms_train"] > 0
+        for a, b in zip(learned, plain):
+            for x, y in zip(a, b):
+                assert np.array_equal(x, y)
     picks = sorted(range(len(small_batch)), key=lambda k: small_batch[k][1].shape[0])[:3]
     for k in picks:
         X, IEN, o, h, N = small_batch[k]
@@ -179,3 +184,22 @@ def test_learned_batch_equals_unbounded_and_oracle(gpu_ctx, small_batch):
         d_ref, _, _ = oracle.distances(X, IEN, o, h, N, mode=2, nodes=nodes)
         assert np.array_equal(dist[nodes], d_ref)
         assert np.array_equal(sign[nodes], oracle.signs(X, IEN, o, h, N, nodes=nodes)["sign"])
+
+
+def test_learned_batch_fallbacks_rerun_in_the_graph(gpu_ctx, small_batch):
+    """The persistent learned batch with a zero search margin: the radius is the network's bare
+    prediction, so many bricks are not certified and rerun in the graph's second launch (the listed
+    plain search); the fields still equal the plain unbounded batch bit for bit."""
+    from stl2sdf import _native
+
+    plain = gpu_ctx.sdf_batch(small_batch, mode=_native.MODE_UNBOUNDED, streams=4, autotune=False, persistent=True)
+    try:
+        gpu_ctx.set_radius_margin(0.0, 0.0)
+        learned = gpu_ctx.sdf_batch(small_batch, mode=_native.MODE_LEARNED, streams=4, autotune=False, persistent=True)
+        st = gpu_ctx.stats()
+    finally:
+        gpu_ctx.set_radius_margin()
+    assert st["unbounded_fallbacks"] > 0.05 * st["ngp"]
+    assert st["certified_nodes"] + st["unbounded_fallbacks"] == st["ngp"]
+    for a, b in zip(learned, plain):
+        assert np.array_equal(a, b)
