@@ -270,16 +270,18 @@ int sdfgpu_autotune(sdfgpu_ctx* ctx, const double origin[3], double h, const int
  * search; no reference counterpart).  A 3 x 64 Fourier-feature MLP (FP16 weights, FP32
  * accumulate) is trained on the GPU on the exact unbounded distances of a coarse grid of the current
  * mesh (coarse_n - 1 cells on the longest axis of the mesh box, padded by one cell).  sdfgpu_distances
- * with use_learned_radius = 1 then bounds each node's search by the predicted radius; a hit inside
- * it is certified exact, other nodes fall back to the unbounded search (stats: certified_nodes,
- * unbounded_fallbacks).  Results are bit-identical to the plain unbounded mode. */
+ * with use_learned_radius = 1 (or SDFGPU_MODE_LEARNED) then predicts a radius at the centre c of
+ * every warp brick and starts the search of each node p of the brick from r(c) + |p - c|; a node
+ * that finds a triangle inside that bound is certified exact, the bricks with other nodes are
+ * searched again without it (stats: certified_nodes, unbounded_fallbacks).  Results are
+ * bit-identical to the plain unbounded mode. */
 int sdfgpu_train_radius(sdfgpu_ctx* ctx, int32_t coarse_n, int32_t steps, int32_t batch, float lr, uint64_t seed,
                         float* final_loss);
 /* Warp brick of the unbounded search: the nodes (brick[0] x brick[1] x brick[2] along x, y, z,
  * product 32) whose nearest triangles one warp searches together.  Default 4 x 2 x 4. */
 int sdfgpu_set_brick(sdfgpu_ctx* ctx, const int32_t brick[3]);
-/* Margin of the learned radius: r = (dhat (1 + alpha) + beta * coarse spacing / s) * s, where dhat is
- * the network's normalised distance and s its normalisation scale.  Defaults alpha = 0.5, beta = 4.
+/* Margin of the learned radius: r = (dhat (1 + alpha) + beta * coarse spacing / s) * s at a brick
+ * centre, where dhat is the network's normalised distance and s its normalisation scale.  Defaults alpha = 0.5, beta = 4.
  * A smaller margin prunes more and certifies fewer nodes; results never change.  alpha = +inf makes
  * every radius infinite: the learned mode's search without the network's bound (to measure what the
  * network gains). */
