@@ -113,18 +113,13 @@ __global__ void __launch_bounds__(kPThreads) k_nearest_points(LearnArgs LA) {
     const float3 p32 = local32(g, p);
     LaneBest L;
     L.m = INFINITY;
-    L.overflow = false;
+    L.occ = 0u;
     L.t = s_keep_t + threadIdx.x;
     L.d = s_keep_d + threadIdx.x;
-#pragma unroll
-    for (int q = 0; q < kKeep; ++q) {
-      L.t[q * kPThreads] = -1;
-      L.d[q * kPThreads] = INFINITY;
-    }
     double m64 = kBig;
     d3 proj = {0.0, 0.0, 0.0};
     bool ok = point_search<false>(LA, p, p32, INFINITY, L, m64, proj, fp64, visits);
-    if (ok && L.overflow) ok = point_search<true>(LA, p, p32, band_of(A, L.m), L, m64, proj, fp64, visits);
+    if (ok && (L.occ & kBandOverflow)) ok = point_search<true>(LA, p, p32, band_of(A, L.m), L, m64, proj, fp64, visits);
     else if (ok) lane_resolve<kPThreads>(A, L, p, m64, proj, fp64);
     if (!ok) ++errs;
     A.dist[lin] = m64;

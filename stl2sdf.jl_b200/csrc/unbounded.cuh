@@ -114,13 +114,16 @@ __device__ __noinline__ void step64_call(const TriRec64* rec, int prim, const d3
 // which is the true (FP64) nearest: |FP32 - FP64| <= err for every distance, so the FP64 winner t*
 // has D32(t*) <= d64(t*) + err <= d64(t_m) + err <= m + 2 err.  The kept triangles live in shared
 // memory (slot q of thread x at q * S + x, S the CTA's thread count: consecutive threads,
-// consecutive banks), which keeps the traversal's registers low.  Free slots hold INF.
+// consecutive banks), which keeps the traversal's registers low; bits 0..7 of occ mark the slots in
+// use (so a new search starts with occ = 0 and no slot needs clearing), bit 8 that the band held
+// more than kKeep triangles at some point.
 constexpr int kUnbThreads = kUnbWarps * 32;
+constexpr unsigned kBandOverflow = 0x100u;
 struct LaneBest {
   float m;
-  bool overflow;  // the band held more than kKeep triangles at some point
-  int* t;         // shared: kept triangle ids
-  float* d;       // shared: their FP32 distances
+  unsigned occ;  // slots in use (bits 0..7), kBandOverflow
+  int* t;        // shared: kept triangle ids
+  float* d;      // shared: their FP32 distances
 };
 
 template <class P>
@@ -131,27 +134,24 @@ __device__ __forceinline__ void lane_offer(const P& A, LaneBest& L, float D, int
   if (D < L.m) {
     L.m = D;
     const float bd = band_of(A, D);
-#pragma unroll
-    for (int q = 0; q < kKeep; ++q)
-      if (L.d[q * S] > bd) L.d[q * S] = INFINITY;
+    for (unsigned o = L.occ & 0xffu; o; o &= o - 1u) {  // drop the kept triangles now outside the band
+      const int q = __ffs(o) - 1;
+      if (L.d[q * S] > bd) L.occ &= ~(1u << q);
+    }
   } else if (D > band_of(A, L.m)) {
     return;
   }
-  int free_q = -1;
-  bool dup = false;
-#pragma unroll
-  for (int q = 0; q < kKeep; ++q) {
-    const float dq = L.d[q * S];
-    if (dq != INFINITY && L.t[q * S] == tri) dup = true;  // already kept (a second pass)
-    if (free_q < 0 && dq == INFINITY) free_q = q;
-  }
-  if (dup) return;
-  if (free_q < 0) {
-    L.overflow = true;
+  for (unsigned o = L.occ & 0xffu; o; o &= o - 1u)
+    if (L.t[(__ffs(o) - 1) * S] == tri) return;  // already kept (a second pass)
+  const unsigned fr = ~L.occ & 0xffu;
+  if (!fr) {
+    L.occ |= kBandOverflow;
     return;
   }
-  L.d[free_q * S] = D;
-  L.t[free_q * S] = tri;
+  const int q = __ffs(fr) - 1;
+  L.d[q * S] = D;
+  L.t[q * S] = tri;
+  L.occ |= 1u << q;
 }
 
 // One warp searches the LBVH for the nearest triangles of its 32 nodes together (a packet
@@ -251,7 +251,7 @@ struct SearchP {
 };
 struct SearchOut {
   float m;         // the lane's FP32 minimum at the end
-  bool overflow;   // its band overflowed
+  unsigned occ;    // its band's slots in use and kBandOverflow
   bool ok;         // the visit and stack bounds held
   int64_t visits;
 };
@@ -259,13 +259,13 @@ __device__ __forceinline__ SearchP search_params(const UnbArgs& A) {
   return SearchP{A.nodes, A.obb, A.ltri, A.rec, A.pad, A.eD_abs, A.eD_rel, A.max_visits};
 }
 // m0: the lane's starting minimum (INFINITY, or a bound it must beat); keep_t / keep_d: its band
-// slots in shared memory (stride S), cleared by the caller.
+// slots in shared memory (stride S), all free at the start.
 template <int S>
 __device__ __noinline__ SearchOut fp32_search(const SearchP A, int* stack, int lane, int rep, float3 p32, bool active,
                                               float m0, int* keep_t, float* keep_d) {
   LaneBest L;
   L.m = m0;
-  L.overflow = false;
+  L.occ = 0u;
   L.t = keep_t;
   L.d = keep_d;
   double m64 = kBig;
@@ -273,7 +273,7 @@ __device__ __noinline__ SearchOut fp32_search(const SearchP A, int* stack, int l
   const d3 p = {0.0, 0.0, 0.0};  // the FP32 pass takes no FP64 step
   int64_t fp64 = 0, visits = 0;
   const bool ok = warp_search<false, S>(A, stack, lane, rep, p, p32, active, INFINITY, L, m64, proj, fp64, visits);
-  return SearchOut{L.m, L.overflow, ok, visits};
+  return SearchOut{L.m, L.occ, ok, visits};
 }
 
 // FP64 steps over the kept triangles inside the final band, in ascending triangle index (so exact
@@ -286,8 +286,8 @@ __device__ __forceinline__ void lane_resolve(const UnbArgs& A, const LaneBest& L
 #pragma unroll 1
   for (int it = 0; it < kKeep; ++it) {
     int best = 0x7fffffff;
-#pragma unroll
-    for (int q = 0; q < kKeep; ++q) {
+    for (unsigned o = L.occ & 0xffu; o; o &= o - 1u) {
+      const int q = __ffs(o) - 1;
       const int tq = L.t[q * S];
       if (L.d[q * S] <= bd && tq > last && tq < best) best = tq;
     }
