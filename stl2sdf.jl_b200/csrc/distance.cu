@@ -537,7 +537,8 @@ __global__ void __launch_bounds__(kUnbThreads, 4) k_unbounded(UnbArgs A) {
   int* stack = s_stack[w];
   const int lx = lane % A.b[0], ly = (lane / A.b[0]) % A.b[1], lz = lane / (A.b[0] * A.b[1]);
   const int rep = A.b[0] / 2 + A.b[0] * (A.b[1] / 2 + A.b[1] * (A.b[2] / 2));
-  int64_t fp64 = 0, errs = 0, visits = 0;
+  // per-thread statistics (32-bit: a thread's totals stay far below 2^32)
+  uint32_t fp64 = 0, errs = 0, visits = 0;
   if (kRadius && lane == 0) s_cf[w][0] = s_cf[w][1] = 0u;
   const int64_t total = kListed ? (int64_t)*A.bricks_n : A.nbricks;
   for (int64_t q = next_brick(A, lane); q < total; q = next_brick(A, lane)) {

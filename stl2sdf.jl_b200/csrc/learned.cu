@@ -28,12 +28,12 @@ constexpr int kTStack = 64;  // per-thread traversal stack (LBVH depth <= 64 for
 
 template <bool kExact>
 __device__ bool point_search(const LearnArgs& LA, const d3& p, const float3& p32, float lim_r, LaneBest& L,
-                             double& m64, d3& proj, int64_t& fp64, int64_t& visits) {
+                             double& m64, d3& proj, uint32_t& fp64, uint32_t& visits) {
   const UnbArgs& A = LA.u;
   int st_id[kTStack];
   float st_d[kTStack];
   int sp = 0, cur = 0;
-  int64_t n = 0;
+  uint32_t n = 0;  // at most max_visits = 2 nel + 64 < 2^30
   auto bound = [&]() -> float {
     if (kExact) {
       const float mf = (float)m64;
@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(kPThreads) k_nearest_points(LearnArgs LA) {
   __shared__ float s_keep_d[kKeep * kPThreads];
   const UnbArgs& A = LA.u;
   const GridP& g = A.g;
-  int64_t fp64 = 0, errs = 0, visits = 0;
+  uint32_t fp64 = 0, errs = 0, visits = 0;  // per-thread statistics (far below 2^32)
   for (int64_t lin = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; lin < g.ngp; lin += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = lin % g.n[0], j = (lin / g.n[0]) % g.n[1], k = lin / (g.n[0] * g.n[1]);
     const d3 p = gnode(g, i, j, k);

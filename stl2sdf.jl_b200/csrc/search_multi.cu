@@ -33,7 +33,7 @@ __global__ void __launch_bounds__(kUnbThreads, 4)
   __shared__ __align__(16) unsigned char s_args_raw[kUnbWarps][sizeof(UnbArgs)];  // the warp's item (raw: no constructor)
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const UnbArgs& args = *reinterpret_cast<const UnbArgs*>(s_args_raw[w]);
-  int64_t fp64 = 0, errs = 0, visits = 0;
+  uint32_t fp64 = 0, errs = 0, visits = 0;  // per-thread statistics (far below 2^32)
   if (kRadius && lane == 0) s_cf[w][0] = s_cf[w][1] = 0u;
   const int64_t total = kListed ? (int64_t)*list_n : off[count];
   int cur = -1, lx = 0, ly = 0, lz = 0, rep = 0;

@@ -164,12 +164,12 @@ __device__ __forceinline__ void lane_offer(const P& A, LaneBest& L, float D, int
 // exceeded.
 template <bool kExact, int S, class P>
 __device__ bool warp_search(const P& A, int* stack, int lane, int rep, const d3& p, const float3& p32,
-                            bool active, float r0, LaneBest& L, double& m64, d3& proj, int64_t& fp64,
-                            int64_t& visits_out) {
+                            bool active, float r0, LaneBest& L, double& m64, d3& proj, uint32_t& fp64,
+                            uint32_t& visits_out) {
   int sp = 1;
   if (lane == 0) stack[0] = 0;
   __syncwarp();
-  int64_t visits = 0;
+  uint32_t visits = 0;  // at most max_visits = 2 nel + 64 < 2^30
   bool ok = true;
   while (sp > 0) {
     if (++visits > A.max_visits) { ok = false; break; }
@@ -253,7 +253,7 @@ struct SearchOut {
   float m;         // the lane's FP32 minimum at the end
   unsigned occ;    // its band's slots in use and kBandOverflow
   bool ok;         // the visit and stack bounds held
-  int64_t visits;
+  uint32_t visits;
 };
 __device__ __forceinline__ SearchP search_params(const UnbArgs& A) {
   return SearchP{A.nodes, A.obb, A.ltri, A.rec, A.pad, A.eD_abs, A.eD_rel, A.max_visits};
@@ -271,7 +271,7 @@ __device__ __noinline__ SearchOut fp32_search(const SearchP A, int* stack, int l
   double m64 = kBig;
   d3 proj = {0.0, 0.0, 0.0};
   const d3 p = {0.0, 0.0, 0.0};  // the FP32 pass takes no FP64 step
-  int64_t fp64 = 0, visits = 0;
+  uint32_t fp64 = 0, visits = 0;
   const bool ok = warp_search<false, S>(A, stack, lane, rep, p, p32, active, INFINITY, L, m64, proj, fp64, visits);
   return SearchOut{L.m, L.occ, ok, visits};
 }
@@ -280,7 +280,7 @@ __device__ __noinline__ SearchOut fp32_search(const SearchP A, int* stack, int l
 // ties keep the lowest index, as a fold in index order does).
 template <int S>
 __device__ __forceinline__ void lane_resolve(const UnbArgs& A, const LaneBest& L, const d3& p, double& m64, d3& proj,
-                                             int64_t& fp64) {
+                                             uint32_t& fp64) {
   const float bd = band_of(A, L.m);
   int last = -1;
 #pragma unroll 1
