@@ -173,3 +173,16 @@ def test_work_model_counts_single_triangle():
     # only the z line through (x, y) inside the box meets it (z = 0.3 / 0.8 is outside [0, 0])
     assert c["nrow"].tolist() == [[0, 0, 1], [0, 0, 1], [0, 0, 1]]
     assert np.all(c["rays"] >= 6)
+
+
+def test_tile_list_model_orders_the_lists():
+    """The tile-list model on the icosphere workload: the least certified list (triangles within
+    d_true(p) of some node) is contained in the perfect-radius ball list, which the default-margin
+    list contains; every list is a count of triangles of the mesh."""
+    import importlib
+
+    r = importlib.import_module("oracle.work_model").tile_lists("icosphere")
+    nel = 5120
+    assert 0 < r["mean_list_union_perfect_radius"] <= r["mean_list_perfect_radius"] <= r["mean_list_default_margin"] <= nel
+    assert 0 < r["mean_list_ref_rule"] <= nel
+    assert r["mean_tile_radius_h"] > 0
