@@ -73,7 +73,6 @@ void add_stats(sdfgpu_stats& a, const sdfgpu_stats& b) {
   a.extra_rays += b.extra_rays;
   a.winding_nodes += b.winding_nodes;
   a.winding_ambiguous += b.winding_ambiguous;
-  a.unbounded_fallbacks += b.unbounded_fallbacks;
   a.rho_max = std::max(a.rho_max, b.rho_max);
   a.ms_distance += b.ms_distance;
   a.ms_sign += b.ms_sign;
