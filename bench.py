@@ -41,7 +41,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "SDF grid nodes/s on 1 B200: learned-radius vs plain GPU vs CPU ref, sign exact"
 L2_NOTE = "a 256 MB device write between timed steps flushes the 126 MB L2 (the mesh records and fields exceed it too)"
-TRAIN = dict(coarse_n=32, steps=200, batch=2048, lr=5e-3, seed=0)  # the learned form's per-mesh training
+TRAIN = dict(coarse_n=24, steps=50, batch=2048, lr=5e-3, seed=0)  # the learned form's per-mesh training
 
 
 def common_config(name, X, IEN, g):

@@ -30,7 +30,7 @@ struct RadiusNorm {
   float alpha = 0.5f;  // radius margin: r = (dhat (1 + alpha) + beta coarse_h / s) s; the fastest
   float beta = 4.0f;   // measured (tighter margins leave nodes uncertified, and those search twice)
   // options of the last training (what a SDFGPU_MODE_LEARNED batch trains every mesh with)
-  int train_coarse = 32, train_steps = 200, train_batch = 2048;
+  int train_coarse = 24, train_steps = 50, train_batch = 2048;
   float train_lr = 5e-3f;
   uint64_t train_seed = 0;
 };

@@ -237,45 +237,6 @@ __device__ bool warp_search(const P& A, int* stack, int lane, int rep, const d3&
   return ok;
 }
 
-// The FP32 pass of the packet search as one out-of-line function, shared by every instantiation of
-// k_unbounded: the hot loop is compiled once, with its own register allocation, whatever the
-// calling kernel keeps live around it.  Its inputs come by value (SearchP: the fields the pass
-// reads) and its results go back by value, so nothing of the lane's state sits in local memory.
-struct SearchP {
-  const BNode* nodes;
-  const OBox* obb;
-  const LeafTri* ltri;
-  const TriRec64* rec;  // not read by the FP32 pass
-  float pad, eD_abs, eD_rel;
-  int64_t max_visits;
-};
-struct SearchOut {
-  float m;         // the lane's FP32 minimum at the end
-  unsigned occ;    // its band's slots in use and kBandOverflow
-  bool ok;         // the visit and stack bounds held
-  uint32_t visits;
-};
-__device__ __forceinline__ SearchP search_params(const UnbArgs& A) {
-  return SearchP{A.nodes, A.obb, A.ltri, A.rec, A.pad, A.eD_abs, A.eD_rel, A.max_visits};
-}
-// m0: the lane's starting minimum (INFINITY, or a bound it must beat); keep_t / keep_d: its band
-// slots in shared memory (stride S), all free at the start.
-template <int S>
-__device__ __noinline__ SearchOut fp32_search(const SearchP A, int* stack, int lane, int rep, float3 p32, bool active,
-                                              float m0, int* keep_t, float* keep_d) {
-  LaneBest L;
-  L.m = m0;
-  L.occ = 0u;
-  L.t = keep_t;
-  L.d = keep_d;
-  double m64 = kBig;
-  d3 proj = {0.0, 0.0, 0.0};
-  const d3 p = {0.0, 0.0, 0.0};  // the FP32 pass takes no FP64 step
-  uint32_t fp64 = 0, visits = 0;
-  const bool ok = warp_search<false, S>(A, stack, lane, rep, p, p32, active, INFINITY, L, m64, proj, fp64, visits);
-  return SearchOut{L.m, L.occ, ok, visits};
-}
-
 // FP64 steps over the kept triangles inside the final band, in ascending triangle index (so exact
 // ties keep the lowest index, as a fold in index order does).
 template <int S>

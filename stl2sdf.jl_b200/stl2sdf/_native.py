@@ -348,7 +348,7 @@ class Context:
         (the learned mode's search without the network's bound)."""
         self._check(lib().sdfgpu_set_radius_margin(self._p, float(alpha), float(beta)))
 
-    def train_radius(self, coarse_n=64, steps=1500, batch=8192, lr=2e-3, seed=0):
+    def train_radius(self, coarse_n=24, steps=50, batch=2048, lr=5e-3, seed=0):
         loss = ctypes.c_float()
         self._check(lib().sdfgpu_train_radius(self._p, int(coarse_n), int(steps), int(batch), float(lr), int(seed),
                                               ctypes.byref(loss)))

@@ -22,7 +22,7 @@ from conftest import grid_of, sample_nodes
 pytestmark = pytest.mark.gpu
 
 DIST_TOL_DIAG = 1e-6  # |d| error bar relative to the bounding-box diagonal (bit-exactness is asserted too)
-TRAIN = dict(coarse_n=32, steps=200, batch=2048, lr=5e-3, seed=0)  # the bench's per-mesh training
+TRAIN = dict(coarse_n=24, steps=50, batch=2048, lr=5e-3, seed=0)  # the bench's per-mesh training
 
 
 def _mesh(name):
