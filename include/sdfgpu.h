@@ -275,7 +275,7 @@ int sdfgpu_autotune(sdfgpu_ctx* ctx, const double origin[3], double h, const int
  * that finds a triangle inside that bound is certified exact, the bricks with other nodes are
  * searched again without it (stats: certified_nodes, unbounded_fallbacks).  Results are
  * bit-identical to the plain unbounded mode.  With the default margin, coarse_n = 24 and 50 Adam
- * steps of 2,048 samples at lr 5e-3 certify every node of 1.4M- and 5.7M-triangle meshes (4 ms of
+ * steps of 2,048 samples at lr 5e-3 certify every node of 1.4M- and 5.7M-triangle meshes (3 ms of
  * training); longer training changes the search time by less than 1%. */
 int sdfgpu_train_radius(sdfgpu_ctx* ctx, int32_t coarse_n, int32_t steps, int32_t batch, float lr, uint64_t seed,
                         float* final_loss);
