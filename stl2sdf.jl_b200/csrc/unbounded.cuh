@@ -151,8 +151,9 @@ __device__ __forceinline__ void lane_offer(const P& A, LaneBest& L, float D, int
   } else if (D > band_of(A, L.m)) {
     return;
   }
-  for (unsigned o = L.occ & 0xffu; o; o &= o - 1u)
-    if (L.t[(__ffs(o) - 1) * S] == tri) return;  // already kept (a second pass)
+  // no duplicate check: a search reaches each leaf at most once (every LBVH node has one parent and
+  // is pushed at most once), every search starts with an empty band, and the FP64 re-search of an
+  // overflowed band takes its FP64 steps without offering
   const unsigned fr = ~L.occ & 0xffu;
   if (!fr) {
     L.occ |= kBandOverflow;
